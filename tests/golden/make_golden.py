@@ -1,0 +1,188 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs only where the reference project is mounted (the survey container): it
+builds oracle/ref_probe (the reference's own host-compilable headers compiled
+in place, outputs into oracle/_ref/) and records their outputs as plain
+numbers.  The fixtures pin the oracle and the product; nothing here runs on
+the GPU box.
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import hashlib
+import json
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def load_probe(ref: str):
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle", "ref_probe"), f"REF={ref}"], check=True)
+    L = C.CDLL(os.path.join(REPO, "oracle", "_ref", "libref_probe.so"))
+    u32, u64, i32, i64, dbl = C.c_uint32, C.c_uint64, C.c_int, C.c_int64, C.c_double
+    sig = {
+        "ref_xxh32_u32": (u32, [u32, u32]), "ref_xxh32_u64": (u32, [u64, u32]),
+        "ref_xxh64_u32": (u64, [u32, u64]), "ref_xxh64_u64": (u64, [u64, u64]),
+        "ref_xxh64_i64": (u64, [i64, u64]), "ref_xxh64_f32": (u64, [C.c_float, u64]),
+        "ref_murmur3_u32": (u32, [u32, u32]), "ref_murmur3_u64": (u32, [u64, u32]),
+        "ref_fmix32": (u32, [u32, u32]), "ref_fmix64": (u64, [u64, u64]),
+        "ref_prime_count": (u64, []), "ref_prime_at": (i64, [u64]),
+        "ref_valid_capacity": (u64, [u64, i32, i32]),
+        "ref_probe_walk": (None, [i32, i32, i32, i32, u64, u32, u32, C.c_void_p]),
+        "ref_bloom_locate": (None, [i32, u64, u64, u64, C.c_void_p, C.c_void_p]),
+        "ref_hll_finalize": (u64, [i32, dbl, i32]),
+        "ref_hll_points": (i32, [i32]), "ref_hll_raw": (dbl, [i32, i32]),
+        "ref_hll_bias": (dbl, [i32, i32]), "ref_hll_threshold": (dbl, [i32]),
+    }
+    for n, (r, a) in sig.items():
+        f = getattr(L, n)
+        f.restype, f.argtypes = r, a
+    return L
+
+
+def edge_keys(rng, nbytes):
+    m = (1 << (8 * nbytes)) - 1
+    base = [0, 1, 2, 42, 123456789, 0x41424344, m, m - 1, m >> 1, (m >> 1) + 1, 0xdeadbeef & m]
+    return base + [int(x) for x in rng.integers(0, m, size=48, dtype=np.uint64, endpoint=True)]
+
+
+def hashes(L, rng):
+    out = {"known_answers_from_reference_tests": {
+        # tests/utility/hash_test.cpp:17-46
+        "fmix32(0x41424344, seed 0xffffeeee)": 0x570df661,
+        "fmix64(0x41424344, seed 0xffffeeee)": 0x5ee45a8eb612f708,
+        "murmur3_32(0x41424344, seed 0xffffeeee)": 0xd6bdbbb4,
+        "xxh32_u32(123456789, seed 0)": 0xb20a85ee,
+        "xxh32_u32(42, seed 0)": 0x454235d1,
+        # tests/utility/xxhash64_test.cpp:88-98
+        "xxh64_u32(0, seed 0)": 4246796580750024372, "xxh64_u32(0, seed 42)": 3614696996920510707,
+        "xxh64_u32(42, seed 0)": 15516826743637085169, "xxh64_u32(123456789, seed 0)": 9462334144942111946,
+        "xxh64_u64(0, seed 0)": 3803688792395291579, "xxh64_u64(0, seed 42)": 13194218611613725804,
+        "xxh64_u64(42, seed 0)": 13066772586158965587, "xxh64_u64(123456789, seed 0)": 14662639848940634189,
+    }}
+    seeds32 = [0, 1, 42, 0xffffeeee]
+    rows = []
+    for k in edge_keys(rng, 4):
+        for s in seeds32:
+            rows.append({"key_bytes": 4, "key": k, "seed": s,
+                         "xxh32": L.ref_xxh32_u32(k, s), "murmur3_32": L.ref_murmur3_u32(k, s),
+                         "fmix": L.ref_fmix32(k, s), "xxh64": L.ref_xxh64_u32(k, s)})
+    for k in edge_keys(rng, 8):
+        for s in seeds32:
+            rows.append({"key_bytes": 8, "key": k, "seed": s,
+                         "xxh32": L.ref_xxh32_u64(k, s), "murmur3_32": L.ref_murmur3_u64(k, s),
+                         "fmix": L.ref_fmix64(k, s), "xxh64": L.ref_xxh64_u64(k, s)})
+    out["vectors"] = rows
+    # signed and float keys hash their object representation (xxhash.h:177-183)
+    out["xxh64_i64"] = [{"key": int(k), "seed": 0, "h": L.ref_xxh64_i64(int(k), 0)}
+                        for k in [-1, -2, -(1 << 63), (1 << 63) - 1, 0]]
+    out["xxh64_f32"] = [{"bits": b, "seed": 0,
+                         "h": L.ref_xxh64_f32(np.array([b], np.uint32).view(np.float32)[0].item(), 0)}
+                        for b in [0x00000000, 0x80000000, 0x3f800000, 0x7fc00000, 0xff800000]]
+    return out
+
+
+def capacity(L, rng):
+    n = L.ref_prime_count()
+    table = np.array([L.ref_prime_at(i) for i in range(n)], dtype=np.int64)
+    reqs = list(range(0, 300)) + [2 ** e + d for e in range(9, 33) for d in (-1, 0, 1)]
+    reqs += [int(x) for x in rng.integers(300, 2 ** 32, size=300, dtype=np.uint64)]
+    reqs += [2_097_152, 268_435_456, 65_536, 2_048, 8_388_608, 16_666_667, 333_333_334]
+    rows = []
+    for b in (1, 2, 4, 5, 8):
+        for dh in (0, 1):
+            caps = [L.ref_valid_capacity(r, b, dh) for r in reqs]
+            rows.append({"bucket_size": b, "double_hashing": dh, "capacities": caps})
+    too_big = [L.ref_valid_capacity(int(table[-1]) * 5 + 6, 5, 1)]
+    return {
+        "prime_count": int(n),
+        "prime_sha256_le_int64": hashlib.sha256(table.tobytes()).hexdigest(),
+        "prime_first": table[:40].tolist(), "prime_last": table[-5:].tolist(),
+        "prime_sample_index": list(range(0, int(n), 997)),
+        "prime_sample": table[::997].tolist(),
+        "requests": reqs, "tables": rows, "beyond_table_returns_error": too_big,
+    }
+
+
+def probing(L, rng):
+    rows = []
+    for kb in (4, 8):
+        for b in (1, 5, 8):
+            for dh in (0, 1):
+                for hk in (0, 1, 2, 3):
+                    for cap_req in (40, 1000, 2_097_152):
+                        cap = L.ref_valid_capacity(cap_req, b, dh)
+                        for k in edge_keys(rng, kb)[:6]:
+                            buf = (C.c_uint32 * 12)()
+                            L.ref_probe_walk(kb, b, dh, hk, k, cap, 12, buf)
+                            rows.append({"key_bytes": kb, "bucket_size": b, "double_hashing": dh, "hash": hk,
+                                         "capacity": cap, "key": k, "walk": list(buf)})
+    return {"walks": rows}
+
+
+def bloom(L, rng):
+    rows = []
+    for kb in (4, 8):
+        for nb in (1, 7, 1024, 1 << 22, (1 << 32) - 1):
+            for seed in (0, 42):
+                for k in edge_keys(rng, kb)[:20]:
+                    blk = C.c_uint32()
+                    pat = (C.c_uint32 * 8)()
+                    L.ref_bloom_locate(kb, k, nb, seed, C.byref(blk), pat)
+                    rows.append({"key_bytes": kb, "num_blocks": nb, "seed": seed, "key": k,
+                                 "block": blk.value, "patterns": list(pat)})
+    return {"locate": rows}
+
+
+def hll(L, rng):
+    tables = {}
+    cases = []
+    for p in range(13, 19):
+        n = L.ref_hll_points(p)
+        raw = np.array([L.ref_hll_raw(p, i) for i in range(n)], dtype=np.float64)
+        bias = np.array([L.ref_hll_bias(p, i) for i in range(n)], dtype=np.float64)
+        tables[str(p)] = {"points": int(n), "threshold": L.ref_hll_threshold(p),
+                          "sha256_raw_then_bias_f64le": hashlib.sha256(raw.tobytes() + bias.tobytes()).hexdigest()}
+        m = 1 << p
+        # synthetic histograms spanning linear counting, the threshold, the
+        # bias-interpolation band and the plain-HLL range
+        for card in np.unique(np.concatenate([
+                np.geomspace(1, 60 * m, 70).astype(np.int64),
+                rng.integers(int(2.4 * m), int(5.2 * m), size=40)])):
+            reg = np.zeros(m, dtype=np.uint8)
+            keys = rng.integers(0, 2 ** 63 - 1, size=int(card), dtype=np.int64)
+            # registers from the same rule as HyperLogLogRef::Add via the oracle
+            import oracle  # noqa: E402  (repo root on sys.path below)
+            oracle.hll_add(reg, p, keys)
+            hist = oracle.hll_histogram(reg, p)
+            z = float(sum(np.ldexp(float(hist[r]), -r) for r in range(65)))
+            cases.append({"precision": p, "hist": hist.tolist(), "z": z, "v": int(hist[0]),
+                          "estimate": L.ref_hll_finalize(p, z, int(hist[0]))})
+    return {"tables": tables, "finalizer_cases": cases}
+
+
+def main():
+    import sys
+    sys.path.insert(0, REPO)
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    args = ap.parse_args()
+    L = load_probe(args.ref)
+    rng = np.random.default_rng(2026)
+    for name, fn in [("hashes", hashes), ("capacity", capacity), ("probing", probing), ("bloom", bloom),
+                     ("hll", hll)]:
+        data = fn(L, rng)
+        with open(os.path.join(HERE, f"{name}.json"), "w") as f:
+            json.dump(data, f, separators=(",", ":"))
+        print(name, os.path.getsize(os.path.join(HERE, f"{name}.json")), "bytes")
+
+
+if __name__ == "__main__":
+    main()
