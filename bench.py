@@ -1,0 +1,532 @@
+"""Benchmark of the bulk hash-container hot path on B200.
+
+Headline workload (one step = one bulk Find of 2^27 keys):
+    StaticMap<int64_t,int64_t>, requested capacity 2^28 slots (268,728,155 after
+    the prime rule, 4.3 GB of 16-byte pairs), DoubleHashing<xxhash_32>, bucket 5,
+    sentinels -1; filled by InsertAndFind (first-wins) to load factor 0.5 with
+    uniform unique int64 keys plus 10% duplicate keys in the insert stream;
+    queried with 2^27 keys at a 50% hit rate.  Other hit rates, a Zipf(1.1)
+    stream, load factor 0.8 and Insert are reported under "extra".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  --impl reference times the reference algorithm's CPU
+restatement (the reference has no CPU implementation of its own) on the host
+cores, same metric and workload, on a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "ops-collections_b200"))
+
+REQ_CAPACITY = 1 << 28
+N_QUERIES = 1 << 27
+LOAD_FACTOR = 0.5
+DUP_FRACTION = 0.10
+SEED = 2026
+METRIC = "StaticMap Find/Insert Gkeys/s @LF0.5 (% HBM roofline); batched keys/s; p50/p99 lat"
+UNIT = "Gkeys/s"
+WORKLOAD = ("StaticMap<int64,int64> single table, capacity 2^28 requested (268,728,155 slots, 4.3 GB), "
+            "DoubleHashing<xxhash_32> bucket 5, filled by InsertAndFind to LF 0.5 (10% duplicate inserts); "
+            "bulk Find of 2^27 int64 queries at 50% hits")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# seeded synthetic inputs (generated on the device; the same arithmetic on the
+# host for the CPU arm)
+# ---------------------------------------------------------------------------
+
+M64 = (1 << 64) - 1
+
+
+def _to_i64(u: int) -> int:
+    return u - (1 << 64) if u >= (1 << 63) else u
+
+
+def mix64_torch(x):
+    """SplitMix64 finalizer, a bijection on 64-bit words, over int64 tensors."""
+    import torch
+
+    def srl(v, k):  # logical shift right on int64
+        return (v >> k) & ((1 << (64 - k)) - 1)
+
+    x = x + _to_i64(0x9E3779B97F4A7C15)
+    x = (x ^ srl(x, 30)) * _to_i64(0xBF58476D1CE4E5B9)
+    x = (x ^ srl(x, 27)) * _to_i64(0x94D049BB133111EB)
+    return x ^ srl(x, 31)
+
+
+def mix64_np(x: np.ndarray) -> np.ndarray:
+    x = x.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        x = x ^ (x >> np.uint64(31))
+    return x.view(np.int64)
+
+
+def counters(lo, n, backend):
+    if backend == "torch":
+        import torch
+        return torch.arange(lo, lo + n, dtype=torch.int64, device="cuda")
+    return np.arange(lo, lo + n, dtype=np.int64)
+
+
+KEY_STREAM, MISS_STREAM, VALUE_STREAM = 0, 1 << 40, 2 << 40
+
+
+def workload_sizes(capacity: int, lf: float):
+    unique = int(math.floor(lf * capacity))
+    dups = int(round(unique * DUP_FRACTION / (1.0 - DUP_FRACTION)))
+    return unique, dups
+
+
+def make_insert_stream(unique, dups, backend):
+    """Unique keys (bijective mix of a counter: distinct, uniform, never -1 in practice)
+    followed by duplicates of earlier keys, shuffled; values are another mixed stream."""
+    if backend == "torch":
+        import torch
+        g = torch.Generator(device="cuda").manual_seed(SEED)
+        keys = mix64_torch(counters(KEY_STREAM, unique, "torch"))
+        dup_idx = torch.randint(0, unique, (dups,), generator=g, device="cuda")
+        stream = torch.cat([keys, keys[dup_idx]])
+        perm = torch.randperm(stream.numel(), generator=g, device="cuda")
+        stream = stream[perm]
+        vals = mix64_torch(counters(VALUE_STREAM, stream.numel(), "torch"))
+        assert not bool((keys == -1).any())
+        return keys, stream, vals
+    rng = np.random.default_rng(SEED)
+    keys = mix64_np(counters(KEY_STREAM, unique, "np"))
+    dup_idx = rng.integers(0, unique, size=dups)
+    stream = np.concatenate([keys, keys[dup_idx]])
+    rng.shuffle(stream)
+    vals = mix64_np(counters(VALUE_STREAM, len(stream), "np"))
+    return keys, stream, vals
+
+
+def make_queries(keys, n, hit_rate, backend, zipf_s=None):
+    """n queries: hit_rate of them drawn from the inserted keys, the rest from a
+    disjoint stream; shuffled.  With zipf_s, all are hits with Zipf-ranked popularity."""
+    if backend == "torch":
+        import torch
+        g = torch.Generator(device="cuda").manual_seed(SEED + 1)
+        u = keys.numel()
+        if zipf_s is not None:
+            r = torch.rand(n, generator=g, device="cuda", dtype=torch.float64)
+            a = 1.0 - zipf_s
+            rank = torch.floor((1.0 + r * (float(u) ** a - 1.0)) ** (1.0 / a)).to(torch.int64) - 1
+            rank = rank.clamp_(0, u - 1)
+            idx = (rank * 2654435761 + 12345) % u  # seeded permutation: rank -> key
+            return keys[idx]
+        nh = int(round(n * hit_rate))
+        hits = keys[torch.randint(0, u, (nh,), generator=g, device="cuda")]
+        miss = mix64_torch(counters(MISS_STREAM, n - nh, "torch"))
+        q = torch.cat([hits, miss])
+        return q[torch.randperm(n, generator=g, device="cuda")]
+    rng = np.random.default_rng(SEED + 1)
+    u = len(keys)
+    nh = int(round(n * hit_rate))
+    hits = keys[rng.integers(0, u, size=nh)]
+    miss = mix64_np(counters(MISS_STREAM, n - nh, "np"))
+    q = np.concatenate([hits, miss])
+    rng.shuffle(q)
+    return q
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per Find launch from the committed ncu summary, if present."""
+    p = os.path.join(REPO, "profiles", "find_map88_lf05_ncu.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_full_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def dist_setup(gpus):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_gpu(args):
+    import torch
+    import b2co
+    rank, world, local = dist_setup(args.gpus)
+    stream = torch.cuda.current_stream()
+    peak, peak_kind = peaks()
+
+    t = b2co.StaticMap(REQ_CAPACITY, -1, -1, key_dtype=torch.int64, value_dtype=torch.int64, bucket_size=5,
+                       probing=b2co.PROBE_DOUBLE, hash_kind=b2co.HASH_XXH32)
+    cap = t.Capacity()
+    unique, dups = workload_sizes(cap, LOAD_FACTOR)
+    keys, stream_keys, vals = make_insert_stream(unique, dups, "torch")
+    pairs = b2co.pack_pairs(stream_keys, vals)
+    found = torch.empty(stream_keys.numel(), dtype=torch.int64, device="cuda")
+    inserted = torch.empty(stream_keys.numel(), dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    t.InsertAndFindAsync(pairs, found, inserted, mode=b2co.IAF_FIRST_WINS)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fill_ms = e0.elapsed_time(e1)
+    n_inserted = int(inserted.sum().item())
+    assert n_inserted == unique, (n_inserted, unique)
+    del found, inserted
+    log(f"[bench] capacity {cap}, unique {unique}, stream {stream_keys.numel()}, fill {fill_ms:.1f} ms")
+
+    q = make_queries(keys, N_QUERIES, 0.5, "torch")
+    out = torch.empty(N_QUERIES, dtype=torch.int64, device="cuda")
+    if args.shape:
+        lanes, items = (int(x) for x in args.shape.split("x"))
+        t.set_find_shape(lanes, items)
+
+    for _ in range(args.warmup):
+        t.FindAsync(q, out)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            t.FindAsync(q, out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    local_ms = e0.elapsed_time(e1)
+    barrier(world)
+    total_ms = max_over_ranks(local_ms, world)
+    ms_per_step = total_ms / args.steps
+    value = world * N_QUERIES * args.steps / (total_ms / 1e3) / 1e9
+
+    # exact probe-window count of the timed queries and parity on a sample, by
+    # the CPU oracle over a host copy of the very same table
+    extra = {}
+    windows_mean, cpu = None, None
+    if rank == 0:
+        windows_mean, cpu, parity = host_side_checks(t, q, out, args)
+        extra["oracle_parity_sample"] = parity
+    bytes_per_query = 8 + 8 + 80 * (windows_mean if windows_mean else 1.0)
+    achieved = N_QUERIES * bytes_per_query / (ms_per_step / 1e3) / 1e9
+    traffic = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_source": peak_kind, "bytes_per_query": round(bytes_per_query, 3),
+                "windows_per_query": windows_mean,
+                "one_window_bound_gbs": round(N_QUERIES * 96 / (ms_per_step / 1e3) / 1e9, 1)}
+
+    # end to end through the C ABI with pinned host buffers
+    hq = q.cpu().pin_memory()
+    ho = torch.empty(N_QUERIES, dtype=torch.int64).pin_memory()
+    t.FindHost(hq.numpy(), ho.numpy())
+    torch.cuda.synchronize()
+    e2e_steps = max(3, min(args.steps, 10))
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        t.FindHost(hq.numpy(), ho.numpy())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e2e_steps
+    assert torch.equal(ho, out.cpu()), "host-buffer Find differs from device Find"
+    e2e = {"value": round(world * N_QUERIES / (e2e_ms / 1e3) / 1e9, 4), "unit": UNIT,
+           "h2d_bytes_per_step": N_QUERIES * 8, "d2h_bytes_per_step": N_QUERIES * 8,
+           "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 24) - 1) >> 24}
+
+    if not args.quick:
+        extra.update(extra_measurements(t, keys, q, out, stream, args))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "capacity": cap, "unique_keys": unique, "insert_stream": unique + dups,
+                       "queries": N_QUERIES, "hit_rate": 0.5, "bucket_size": 5, "probing": "DoubleHashing<xxhash_32>",
+                       "l2": "inputs larger than L2 (4.3 GB table + 1 GB keys)", "parallelism": f"replicas x{world}",
+                       "find_shape": args.shape or "default"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
+            "clocks": clk.summary(), "fill_ms": round(fill_ms, 2), "extra": extra,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def host_side_checks(t, q, out, args):
+    """Probe windows per query (exact, oracle over the device table's bytes),
+    an oracle parity sample and the CPU baseline on the host cores."""
+    import oracle
+    import torch
+    t0 = time.perf_counter()
+    o = oracle.Table(np.int64, np.int64, t.Capacity(), 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, -1, -1)
+    o.load_slots(t.dump_slots())
+    log(f"[bench] table copied to host in {time.perf_counter() - t0:.1f} s")
+    sample = 1 << 22
+    qs = q[:sample].cpu().numpy()
+    exp, win = o.find(qs)
+    parity = {"queries": sample, "identical": bool(np.array_equal(exp, out[:sample].cpu().numpy()))}
+    windows_mean = float(win.mean())
+    cpu = None
+    if not args.no_cpu:
+        threads = os.cpu_count() or 1
+        qa = q.cpu().numpy()
+        done, t0 = 0, time.perf_counter()
+        chunk = 1 << 22
+        while done < len(qa) and time.perf_counter() - t0 < args.cpu_seconds:
+            o.find_parallel(qa[done:done + chunk], threads)
+            done += chunk
+        el = time.perf_counter() - t0
+        cpu = {"value": round(done / el / 1e9, 5), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{done} of the 2^27 timed queries (50% hits) over a host copy of the same LF0.5 table, "
+                         f"oracle Find on {threads} OpenMP threads, {el:.1f} s"}
+    return windows_mean, cpu, parity
+
+
+def extra_measurements(t, keys, q50, out, stream, args):
+    """Secondary numbers: other hit rates, Zipf, contains, insert, LF 0.8."""
+    import torch
+    import b2co
+    res = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    for hr in (0.0, 1.0):
+        qq = make_queries(keys, N_QUERIES, hr, "torch")
+        ms = timed(lambda: t.FindAsync(qq, out))
+        res[f"find_hit{int(hr * 100)}_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
+        del qq
+    qz = make_queries(keys, N_QUERIES, 1.0, "torch", zipf_s=1.1)
+    ms = timed(lambda: t.FindAsync(qz, out))
+    res["find_zipf1.1_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
+    del qz
+    c = torch.empty(N_QUERIES, dtype=torch.uint8, device="cuda")
+    ms = timed(lambda: t.ContainsAsync(q50, c))
+    res["contains_hit50_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
+    del c
+    # Insert: unique pairs into a cleared table (clear not timed)
+    cap = t.Capacity()
+    unique, _ = workload_sizes(cap, LOAD_FACTOR)
+    pairs = b2co.pack_pairs(keys, mix64_torch(counters(VALUE_STREAM, unique, "torch")))
+    tot = 0.0
+    for _ in range(3):
+        t.Clear()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t.InsertAsync(pairs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    res["insert_lf05_gkeys"] = round(unique / (tot / 3) / 1e6, 3)
+    # LF 0.8: refill, Find at 50% hits
+    u8, d8 = workload_sizes(cap, 0.8)
+    t.Clear()
+    k8, s8, v8 = make_insert_stream(u8, d8, "torch")
+    p8 = b2co.pack_pairs(s8, v8)
+    f8 = torch.empty(s8.numel(), dtype=torch.int64, device="cuda")
+    i8 = torch.empty(s8.numel(), dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    e0.record(stream)
+    t.InsertAndFindAsync(p8, f8, i8, mode=b2co.IAF_FIRST_WINS)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    res["insert_and_find_fill_lf08_gkeys"] = round(s8.numel() / e0.elapsed_time(e1) / 1e6, 3)
+    del p8, f8, i8, s8, v8
+    q8 = make_queries(k8, N_QUERIES, 0.5, "torch")
+    ms = timed(lambda: t.FindAsync(q8, out))
+    res["find_lf08_hit50_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
+    return res
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference algorithm's CPU restatement on the host cores
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return  # rank 0 alone times the host-CPU reference
+    import oracle
+    threads = os.cpu_count() or 1
+    cap = oracle.valid_capacity(REQ_CAPACITY, 5, oracle.PROBE_DOUBLE)
+    unique, dups = workload_sizes(cap, LOAD_FACTOR)
+    t0 = time.perf_counter()
+    keys, stream_keys, vals = make_insert_stream(unique, dups, "np")
+    o = oracle.Table(np.int64, np.int64, cap, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, -1, -1)
+    o.insert(stream_keys, vals)  # sequential first-wins fill (same stored set as InsertAndFind)
+    del stream_keys, vals
+    log(f"[reference] host table built in {time.perf_counter() - t0:.1f} s")
+    q = make_queries(keys, N_QUERIES, 0.5, "np")
+    sample = 1 << 24
+    for s in range(args.warmup):
+        o.find_parallel(q[(s * sample) % N_QUERIES:][:sample], threads)
+    times = []
+    for s in range(args.steps):
+        off = (s * sample) % N_QUERIES
+        t0 = time.perf_counter()
+        o.find_parallel(q[off:off + sample], threads)
+        times.append(time.perf_counter() - t0)
+    ms_per_step = 1e3 * float(np.mean(times))
+    value = sample / (ms_per_step / 1e3) / 1e9
+    desc = (f"oracle port of the reference Find (same hash, probing, capacity, bucket scan), {threads} OpenMP "
+            f"threads, {sample} queries per step of the 2^27 50%-hit stream over the LF0.5 table")
+    line = {
+        "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
+        "config": {"workload": WORKLOAD, "capacity": cap, "unique_keys": unique, "queries_per_step": sample},
+        "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b2co", choices=["b2co", "reference"])
+    ap.add_argument("--shape", default="", help="Find kernel shape LANESxITEMS, e.g. 8x1")
+    ap.add_argument("--quick", action="store_true", help="skip the secondary measurements")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

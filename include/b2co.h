@@ -1,0 +1,264 @@
+/*
+ * b2co.h -- C ABI of the B200 bulk-container library (libb2co.so).
+ *
+ * This is the drop-in boundary for the ops-collections bulk-container hot
+ * path.  The reference's boundary is its header-only C++ class-template API
+ * (StaticMap, StaticSet, DynamicMap, BloomFilter, HyperLogLog); every entry
+ * point below replaces one of those methods and cites it as
+ * `reference: <file>:<line>`.  The C++ mirror of the class templates lives in
+ * include/b2co/ and is a thin layer over these functions.
+ *
+ * Conventions (all from the reference's host layer):
+ *   - every function returns a b2co_status; the message of the last failure on
+ *     the calling thread is available from b2co_last_error();
+ *   - data pointers are caller-owned DEVICE pointers unless a name says
+ *     "host"; "pairs" are arrays of the table's slot type (Pair<K,V>, aligned
+ *     to min(16, bitceil(sizeof K + sizeof V)); a bare key for sets);
+ *   - stencils are device uint8 arrays; a nonzero byte selects the item (the
+ *     C ABI carries the `u8 != 0` predicate; AlwaysTrue is a NULL stencil);
+ *   - `*_async` calls are stream-ordered and return after the launch; the
+ *     other calls synchronize the stream, like the reference's sync methods;
+ *   - n == 0 is a no-op; a NULL data pointer with n > 0 makes a sync Insert
+ *     report all n items as failed and an async call a no-op, exactly as
+ *     detail/open_addressing/open_addressing_impl.h:176-201 does;
+ *   - batches beyond the 32-bit index range fail with B2CO_ERANGE
+ *     (open_addressing_impl.h:534-545 throws std::length_error).
+ */
+#ifndef B2CO_H
+#define B2CO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* b2co_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+typedef enum {
+    B2CO_OK = 0,
+    B2CO_EINVAL = 1,   /* std::invalid_argument in the reference */
+    B2CO_ERANGE = 2,   /* std::length_error */
+    B2CO_ENOMEM = 3,   /* std::bad_alloc */
+    B2CO_ECUDA = 4,    /* std::runtime_error: a CUDA call failed */
+    B2CO_ETIMEOUT = 5, /* a bounded device-side wait expired (no reference counterpart) */
+    B2CO_ELOGIC = 6    /* std::logic_error: moved-from / storage-less object */
+} b2co_status;
+
+typedef enum { B2CO_HASH_XXH32 = 0, B2CO_HASH_MURMUR3_32 = 1, B2CO_HASH_FMIX = 2, B2CO_HASH_XXH64 = 3 } b2co_hash;
+typedef enum { B2CO_PROBE_LINEAR = 0, B2CO_PROBE_DOUBLE = 1 } b2co_probing;
+typedef enum {
+    B2CO_IAF_RACE = 0,       /* reference semantics: concurrent duplicates race for the slot */
+    B2CO_IAF_FIRST_WINS = 1  /* deterministic: the first occurrence in input order wins */
+} b2co_iaf_mode;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* b2co_last_error(void);
+const char* b2co_status_string(int status);
+/* Library version string. */
+const char* b2co_version(void);
+
+/* ===================================================================== */
+/* Open-addressing tables: StaticMap<K,T> and StaticSet<K>                 */
+/* ===================================================================== */
+
+typedef struct {
+    uint32_t key_bytes;        /* 4 or 8 */
+    uint32_t value_bytes;      /* 0 = StaticSet, else 4 or 8 */
+    uint32_t bucket_size;      /* Storage<B>: 1, 2, 4, 5 or 8 */
+    uint32_t probing;          /* b2co_probing */
+    uint32_t hash;             /* b2co_hash used by the probing scheme */
+    uint32_t reserved;         /* must be 0 */
+    uint64_t empty_key_bits;   /* sentinel bit patterns (low key_bytes / value_bytes bytes) */
+    uint64_t empty_value_bits;
+    uint64_t erased_key_bits;  /* tombstone key; equal to empty_key_bits = no tombstone */
+} b2co_oa_desc;
+
+typedef struct b2co_oa_table b2co_oa_table;
+
+/* Capacity the table gets for a requested slot count.
+ * reference: include/detail/extent/extent.inl:20-62 (MakeValidExtent). */
+int b2co_oa_valid_capacity(uint64_t requested, uint32_t bucket_size, uint32_t probing, uint64_t* capacity);
+
+/* Allocate and clear a table.
+ * reference: include/static_map.h:78-84, include/static_set.h:73-79,
+ * detail/static_map/static_map.inl:20-36, open_addressing_impl.h:69-93. */
+int b2co_oa_create(const b2co_oa_desc* desc, uint64_t requested_capacity, b2co_stream stream, b2co_oa_table** out);
+/* reference: StaticMap destructor (bucket_storage.h:116-119 frees the slots). */
+int b2co_oa_destroy(b2co_oa_table* table);
+/* reference: static_map.h:584 Capacity(). */
+int b2co_oa_capacity(const b2co_oa_table* table, uint64_t* capacity);
+/* Raw device slots.  reference: static_map.h:604 Data(). */
+int b2co_oa_data(const b2co_oa_table* table, void** slots);
+/* reference: static_map.h:97 SetErasedKey (static_map.inl:59-66). */
+int b2co_oa_set_erased_key(b2co_oa_table* table, uint64_t erased_key_bits, b2co_stream stream);
+/* reference: static_map.h:318 Clear, :331 ClearAsync. */
+int b2co_oa_clear(b2co_oa_table* table, b2co_stream stream);
+int b2co_oa_clear_async(b2co_oa_table* table, b2co_stream stream);
+
+/* Insert (returns the failed count: empty keys, duplicates, full table).
+ * reference: static_map.h:116 Insert, static_map.h:131 InsertAsync,
+ * open_addressing_impl.h:102-110, kernels.h:46-114. */
+int b2co_oa_insert(b2co_oa_table* table, const void* pairs, uint64_t n, b2co_stream stream, uint64_t* failed);
+int b2co_oa_insert_async(b2co_oa_table* table, const void* pairs, uint64_t n, b2co_stream stream);
+/* InsertIf: only stencil-selected items; failed counts selected items only.
+ * reference: static_map.h:216 InsertIf, :237 InsertIfAsync (open_addressing_impl.h:176-218). */
+int b2co_oa_insert_if(b2co_oa_table* table, const void* pairs, const uint8_t* stencil, uint64_t n,
+                      b2co_stream stream, uint64_t* failed);
+int b2co_oa_insert_if_async(b2co_oa_table* table, const void* pairs, const uint8_t* stencil, uint64_t n,
+                            b2co_stream stream);
+/* InsertOrAssign: failed and assigned (existing keys overwritten) counts.
+ * reference: static_map.h:151-175, open_addressing_impl.h:112-156, kernels.h:116-182. */
+int b2co_oa_insert_or_assign(b2co_oa_table* table, const void* pairs, uint64_t n, b2co_stream stream,
+                             uint64_t* failed, uint64_t* assigned);
+int b2co_oa_insert_or_assign_async(b2co_oa_table* table, const void* pairs, uint64_t n, b2co_stream stream);
+/* AssignIfAsync: overwrite payloads of existing selected keys, never insert.
+ * reference: static_map.h:189, open_addressing_impl.h:158-174, open_addressing_ref_impl.h:384-410. */
+int b2co_oa_assign_if_async(b2co_oa_table* table, const void* pairs, const uint8_t* stencil, uint64_t n,
+                            b2co_stream stream);
+/* InsertAndFind: per input the found payload (T[n]; the key for sets) and a
+ * 1-byte inserted flag.
+ * reference: static_map.h:256 InsertAndFind, :273 InsertAndFindAsync, open_addressing_impl.h:220-234, kernels.h:212-245. */
+int b2co_oa_insert_and_find(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
+                            uint64_t n, int mode, b2co_stream stream);
+int b2co_oa_insert_and_find_async(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
+                                  uint64_t n, int mode, b2co_stream stream);
+/* Erase (returns the count of keys not erased).
+ * reference: static_map.h:292 Erase, :307 EraseAsync, open_addressing_impl.h:236-276, open_addressing_ref_impl.h:340-379. */
+int b2co_oa_erase(b2co_oa_table* table, const void* keys, uint64_t n, b2co_stream stream, uint64_t* failed);
+int b2co_oa_erase_async(b2co_oa_table* table, const void* keys, uint64_t n, b2co_stream stream);
+/* Find / FindIf: out[i] = payload of keys[i] or the empty payload.
+ * reference: static_map.h:350 Find, :369 FindAsync, :395 FindIf, :419 FindIfAsync, open_addressing_impl.h:278-299, kernels.h:313-347. */
+int b2co_oa_find(b2co_oa_table* table, const void* keys, void* out, uint64_t n, b2co_stream stream);
+int b2co_oa_find_async(b2co_oa_table* table, const void* keys, void* out, uint64_t n, b2co_stream stream);
+int b2co_oa_find_if(b2co_oa_table* table, const void* keys, const uint8_t* stencil, void* out, uint64_t n,
+                    b2co_stream stream);
+int b2co_oa_find_if_async(b2co_oa_table* table, const void* keys, const uint8_t* stencil, void* out, uint64_t n,
+                          b2co_stream stream);
+/* Contains / ContainsIf: 1-byte bool per key.
+ * reference: static_map.h:439 Contains, :459 ContainsAsync, :485 ContainsIf, :509 ContainsIfAsync, open_addressing_impl.h:301-322, kernels.h:349-377. */
+int b2co_oa_contains(b2co_oa_table* table, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+int b2co_oa_contains_async(b2co_oa_table* table, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+int b2co_oa_contains_if(b2co_oa_table* table, const void* keys, const uint8_t* stencil, uint8_t* out, uint64_t n,
+                        b2co_stream stream);
+int b2co_oa_contains_if_async(b2co_oa_table* table, const void* keys, const uint8_t* stencil, uint8_t* out,
+                              uint64_t n, b2co_stream stream);
+/* Count: number of keys contained.
+ * reference: static_map.h:575, open_addressing_impl.h:446-474, kernels.h:427-467. */
+int b2co_oa_count(b2co_oa_table* table, const void* keys, uint64_t n, b2co_stream stream, uint64_t* count);
+/* Find with HOST key and output buffers: the batch is split into chunks whose
+ * copies in and out overlap the probing on two extra streams.  Same results
+ * as b2co_oa_find; the end-to-end form of the reference's Find for callers
+ * whose data lives in host memory.
+ * reference: static_map.h:350 Find (host staging is the caller's job there). */
+int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_out, uint64_t n,
+                      b2co_stream stream);
+
+/* Kernel shape used by Find/Contains on this table: lanes per key (1, 2, 4 or
+ * 8) and keys per lane per pass (1, 2 or 4); 0 = library default.  The
+ * autotuner sets these.  No reference counterpart (the reference launches one
+ * thread per key). */
+int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_lane);
+
+/* ===================================================================== */
+/* BloomFilter<Key>, default policy (8 x uint32 words per block, xxh64)     */
+/* ===================================================================== */
+
+typedef struct b2co_bloom b2co_bloom;
+
+/* reference: include/bloom_filter.h:59-62, bloom_filter_lifecycle.inl:15-52
+ * (numBlocks 0 -> EINVAL, > UINT32_MAX -> ERANGE). */
+int b2co_bloom_create(uint64_t num_blocks, uint32_t key_bytes, uint64_t seed, b2co_stream stream, b2co_bloom** out);
+int b2co_bloom_destroy(b2co_bloom* filter);
+int b2co_bloom_data(const b2co_bloom* filter, uint32_t** words);
+int b2co_bloom_num_blocks(const b2co_bloom* filter, uint64_t* num_blocks);
+/* reference: bloom_filter.h:66-67 Clear / ClearAsync. */
+int b2co_bloom_clear(b2co_bloom* filter, b2co_stream stream);
+int b2co_bloom_clear_async(b2co_bloom* filter, b2co_stream stream);
+/* reference: bloom_filter.h:69-72 Add / AddAsync / AddIf / AddIfAsync
+ * (bloom_filter_impl.h:40-47, bloom_filter_add.inl:15-89). */
+int b2co_bloom_add(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream stream);
+int b2co_bloom_add_async(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream stream);
+int b2co_bloom_add_if(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint64_t n, b2co_stream stream);
+int b2co_bloom_add_if_async(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint64_t n,
+                            b2co_stream stream);
+/* reference: bloom_filter.h:74-81 Contains / ContainsAsync / ContainsIf
+ * (bloom_filter_query.inl:15-120, bloom_filter_impl.h:49-56). */
+int b2co_bloom_contains(b2co_bloom* filter, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+int b2co_bloom_contains_async(b2co_bloom* filter, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+int b2co_bloom_contains_if(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint8_t* out, uint64_t n,
+                           b2co_stream stream);
+int b2co_bloom_contains_if_async(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint8_t* out,
+                                 uint64_t n, b2co_stream stream);
+/* reference: bloom_filter.h:83-87 Merge / MergeAsync / Intersect / IntersectAsync
+ * (bloom_filter_merge.inl:15-69; incompatible filters -> EINVAL, bloom_filter_query.inl:197-215). */
+int b2co_bloom_merge(b2co_bloom* filter, const b2co_bloom* other, b2co_stream stream);
+int b2co_bloom_merge_async(b2co_bloom* filter, const b2co_bloom* other, b2co_stream stream);
+int b2co_bloom_intersect(b2co_bloom* filter, const b2co_bloom* other, b2co_stream stream);
+int b2co_bloom_intersect_async(b2co_bloom* filter, const b2co_bloom* other, b2co_stream stream);
+
+/* ===================================================================== */
+/* HyperLogLog<Key> (int32 / int64 keys, precision 13..18)                 */
+/* ===================================================================== */
+
+typedef struct b2co_hll b2co_hll;
+
+/* reference: include/hyperloglog.h:28-30, hyperloglog.inl:115-141
+ * (CreateWithSketchSizeKB / CreateWithPrecision / CreateWithStandardDeviation). */
+int b2co_hll_precision_for_sketch_kb(uint32_t sketch_kb, uint32_t* precision);
+int b2co_hll_precision_for_deviation(double deviation, uint32_t* precision);
+int b2co_hll_create(uint32_t precision, uint32_t key_bytes, b2co_stream stream, b2co_hll** out);
+int b2co_hll_destroy(b2co_hll* sketch);
+/* Registers: 2^precision bytes, register i at byte i.  reference: hyperloglog.h:42 Data(). */
+int b2co_hll_data(const b2co_hll* sketch, const uint8_t** registers);
+int b2co_hll_precision(const b2co_hll* sketch, uint32_t* precision);
+/* reference: hyperloglog.h:37-40 Clear / Add / Merge / Estimate
+ * (hyperloglog.inl:215-345). */
+int b2co_hll_clear(b2co_hll* sketch, b2co_stream stream);
+int b2co_hll_add(b2co_hll* sketch, const void* keys, uint64_t n, b2co_stream stream);
+int b2co_hll_add_async(b2co_hll* sketch, const void* keys, uint64_t n, b2co_stream stream);
+int b2co_hll_merge(b2co_hll* sketch, const b2co_hll* other, b2co_stream stream);
+int b2co_hll_estimate(const b2co_hll* sketch, b2co_stream stream, uint64_t* estimate);
+/* The 65-bin rank histogram Estimate reduces (hyperloglog.inl:327-338). */
+int b2co_hll_histogram(const b2co_hll* sketch, b2co_stream stream, uint32_t* host_hist65);
+/* HLL++ finalizer on a histogram (detail/hyperloglog/finalizer.h:46-74). */
+int b2co_hll_finalize(uint32_t precision, const uint32_t* hist65, uint64_t* estimate);
+/* The finalizer's interpolation data for a precision (read-only views). */
+int b2co_hll_bias_data(uint32_t precision, const double** raw_estimates, const double** biases, uint32_t* points,
+                       double* threshold);
+
+/* ===================================================================== */
+/* DynamicMap<K,T>: growing set of StaticMap submaps                        */
+/* ===================================================================== */
+
+typedef struct b2co_dmap b2co_dmap;
+
+/* reference: include/dynamic_map.h:94-133 (emptyKey == erasedKey -> EINVAL). */
+int b2co_dmap_create(const b2co_oa_desc* desc, uint64_t initial_capacity, b2co_stream stream, b2co_dmap** out);
+int b2co_dmap_destroy(b2co_dmap* map);
+/* reference: dynamic_map.h:137-139 Size / Capacity / NumSubmaps. */
+int b2co_dmap_size(const b2co_dmap* map, uint64_t* size);
+int b2co_dmap_capacity(const b2co_dmap* map, uint64_t* capacity);
+int b2co_dmap_num_submaps(const b2co_dmap* map, uint64_t* count);
+/* reference: dynamic_map.h:142-166 Reserve. */
+int b2co_dmap_reserve(b2co_dmap* map, uint64_t n, b2co_stream stream);
+/* Insert returns the number inserted; mode 0 = kExactDedup, 1 = kAppendUnique.
+ * reference: dynamic_map.h:168-219. */
+int b2co_dmap_insert(b2co_dmap* map, const void* pairs, uint64_t n, int mode, b2co_stream stream,
+                     uint64_t* inserted);
+/* InsertOrAssign returns the number of NEW keys (assignments are not counted).
+ * reference: dynamic_map.h:237-260, :549-575. */
+int b2co_dmap_insert_or_assign(b2co_dmap* map, const void* pairs, uint64_t n, b2co_stream stream, uint64_t* done);
+/* reference: dynamic_map.h:262-316 Find / Contains. */
+int b2co_dmap_find(b2co_dmap* map, const void* keys, void* out, uint64_t n, b2co_stream stream);
+int b2co_dmap_contains(b2co_dmap* map, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+/* reference: dynamic_map.h:318-347 Erase (returns the count erased). */
+int b2co_dmap_erase(b2co_dmap* map, const void* keys, uint64_t n, b2co_stream stream, uint64_t* erased);
+/* reference: dynamic_map.h:349-357 Clear. */
+int b2co_dmap_clear(b2co_dmap* map, b2co_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B2CO_H */

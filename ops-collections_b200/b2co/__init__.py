@@ -1,0 +1,570 @@
+"""Python host layer over libb2co.so, mirroring the reference's container API.
+
+The reference (ops-collections) exposes C++ class templates -- StaticMap,
+StaticSet, DynamicMap, BloomFilter, HyperLogLog -- whose methods take device
+pointers, a count and a stream.  These classes keep the same method names,
+argument meaning and error behaviour, over the C ABI declared in
+include/b2co.h.  Device buffers are torch CUDA tensors (plumbing only); every
+operation runs in libb2co's own sm_100a kernels.  There is no CPU fallback:
+without the built library every call raises.
+
+Exceptions map the reference's C++ exceptions:
+    std::invalid_argument -> InvalidArgument (ValueError)
+    std::length_error     -> LengthError (ValueError)
+    std::bad_alloc        -> BadAlloc (MemoryError)
+    std::runtime_error    -> CudaError (RuntimeError)
+    std::logic_error      -> LogicError (RuntimeError)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libb2co.so")
+
+OK, EINVAL, ERANGE, ENOMEM, ECUDA, ETIMEOUT, ELOGIC = range(7)
+HASH_XXH32, HASH_MURMUR3_32, HASH_FMIX, HASH_XXH64 = range(4)
+PROBE_LINEAR, PROBE_DOUBLE = 0, 1
+IAF_RACE, IAF_FIRST_WINS = 0, 1
+INSERT_EXACT_DEDUP, INSERT_APPEND_UNIQUE = 0, 1
+
+
+class B2coError(Exception):
+    status = -1
+
+
+class InvalidArgument(B2coError, ValueError):
+    status = EINVAL
+
+
+class LengthError(B2coError, ValueError):
+    status = ERANGE
+
+
+class BadAlloc(B2coError, MemoryError):
+    status = ENOMEM
+
+
+class CudaError(B2coError, RuntimeError):
+    status = ECUDA
+
+
+class TimeoutError_(B2coError, RuntimeError):
+    status = ETIMEOUT
+
+
+class LogicError(B2coError, RuntimeError):
+    status = ELOGIC
+
+
+_EXC = {EINVAL: InvalidArgument, ERANGE: LengthError, ENOMEM: BadAlloc, ECUDA: CudaError,
+        ETIMEOUT: TimeoutError_, ELOGIC: LogicError}
+
+
+class OaDesc(C.Structure):
+    _fields_ = [("key_bytes", C.c_uint32), ("value_bytes", C.c_uint32), ("bucket_size", C.c_uint32),
+                ("probing", C.c_uint32), ("hash", C.c_uint32), ("reserved", C.c_uint32),
+                ("empty_key_bits", C.c_uint64), ("empty_value_bits", C.c_uint64),
+                ("erased_key_bits", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libb2co.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libb2co.so is not built ({LIB_PATH}); run ops-collections_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        L.b2co_last_error.restype = C.c_char_p
+        L.b2co_status_string.restype = C.c_char_p
+        L.b2co_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(status: int):
+    if status != OK:
+        msg = lib().b2co_last_error().decode(errors="replace")
+        raise _EXC.get(status, B2coError)(msg or lib().b2co_status_string(status).decode())
+
+
+def _call(name, *args):
+    _check(getattr(lib(), name)(*args))
+
+
+def _ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    if t is None:
+        return None
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream):
+    """A cudaStream_t handle: a torch.cuda.Stream, a raw int handle, or None for torch's current stream."""
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _bits(x, nbytes: int) -> int:
+    if isinstance(x, float):
+        fmt = {4: np.float32, 8: np.float64}[nbytes]
+        return int(np.array([x], dtype=fmt).view({4: np.uint32, 8: np.uint64}[nbytes])[0])
+    return int(x) & ((1 << (8 * nbytes)) - 1)
+
+
+def slot_bytes(key_bytes: int, value_bytes: int) -> int:
+    if value_bytes == 0:
+        return key_bytes
+    return 8 if key_bytes + value_bytes == 8 else 16
+
+
+def pack_pairs(keys, values):
+    """Device array of Pair<K,V> slots (the reference's `values` argument) from key and payload tensors."""
+    import torch
+    kb, vb = keys.element_size(), values.element_size()
+    n = keys.numel()
+    if kb == 4 and vb == 4:
+        return torch.stack([keys.view(torch.int32), values.view(torch.int32)], dim=1).contiguous()
+    out = torch.zeros((n, 2), dtype=torch.int64, device=keys.device)
+    if kb == 8:
+        out[:, 0] = keys.view(torch.int64)
+    else:
+        out[:, 0] = keys.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    if vb == 8:
+        out[:, 1] = values.view(torch.int64)
+    else:
+        out[:, 1] = values.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
+    return out
+
+
+def valid_capacity(requested: int, bucket_size: int = 5, probing: int = PROBE_DOUBLE) -> int:
+    c = C.c_uint64()
+    _call("b2co_oa_valid_capacity", C.c_uint64(requested), C.c_uint32(bucket_size), C.c_uint32(probing),
+          C.byref(c))
+    return c.value
+
+
+def _dtype_bytes(dt) -> int:
+    import torch
+    return torch.empty((), dtype=dt).element_size()
+
+
+class _OaBase:
+    """Shared implementation of StaticMap and StaticSet (OpenAddressingImpl)."""
+
+    def __init__(self, capacity, empty_key, empty_value, key_dtype, value_dtype, bucket_size, probing, hash_kind,
+                 erased_key, stream):
+        import torch
+        self.key_dtype = key_dtype
+        self.value_dtype = value_dtype
+        kb = _dtype_bytes(key_dtype)
+        vb = 0 if value_dtype is None else _dtype_bytes(value_dtype)
+        self.key_bytes, self.value_bytes = kb, vb
+        self.empty_key, self.empty_value = empty_key, empty_value
+        d = OaDesc(kb, vb, bucket_size, probing, hash_kind, 0, _bits(empty_key, kb),
+                   _bits(empty_value, vb) if vb else 0,
+                   _bits(empty_key if erased_key is None else erased_key, kb))
+        self._desc = d
+        h = C.c_void_p()
+        _call("b2co_oa_create", C.byref(d), C.c_uint64(capacity), _stream(stream), C.byref(h))
+        self._h = h
+        self.bucket_size = bucket_size
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_oa_destroy(h)
+            self._h = None
+
+    # -- properties (static_map.h:584, :604) ---------------------------------
+    def Capacity(self) -> int:
+        c = C.c_uint64()
+        _call("b2co_oa_capacity", self._h, C.byref(c))
+        return c.value
+
+    def Data(self) -> int:
+        p = C.c_void_p()
+        _call("b2co_oa_data", self._h, C.byref(p))
+        return p.value
+
+    def slot_bytes(self) -> int:
+        return slot_bytes(self.key_bytes, self.value_bytes)
+
+    def dump_slots(self) -> np.ndarray:
+        """Raw slot bytes copied to the host (numpy uint8, capacity * slot_bytes)."""
+        return _device_bytes(self.Data(), self.Capacity() * self.slot_bytes())
+
+    def SetErasedKey(self, erased_key, stream=None):
+        _call("b2co_oa_set_erased_key", self._h, C.c_uint64(_bits(erased_key, self.key_bytes)), _stream(stream))
+
+    def Clear(self, stream=None):
+        _call("b2co_oa_clear", self._h, _stream(stream))
+
+    def ClearAsync(self, stream=None):
+        _call("b2co_oa_clear_async", self._h, _stream(stream))
+
+    # -- inserts --------------------------------------------------------------
+    def Insert(self, values, n=None, stream=None) -> int:
+        f = C.c_uint64()
+        _call("b2co_oa_insert", self._h, _ptr(values), C.c_uint64(self._n(values, n)), _stream(stream),
+              C.byref(f))
+        return f.value
+
+    def InsertAsync(self, values, n=None, stream=None):
+        _call("b2co_oa_insert_async", self._h, _ptr(values), C.c_uint64(self._n(values, n)), _stream(stream))
+
+    def InsertIf(self, values, stencil, n=None, stream=None) -> int:
+        f = C.c_uint64()
+        _call("b2co_oa_insert_if", self._h, _ptr(values), _ptr(stencil), C.c_uint64(self._n(values, n)),
+              _stream(stream), C.byref(f))
+        return f.value
+
+    def InsertIfAsync(self, values, stencil, n=None, stream=None):
+        _call("b2co_oa_insert_if_async", self._h, _ptr(values), _ptr(stencil), C.c_uint64(self._n(values, n)),
+              _stream(stream))
+
+    def InsertAndFind(self, values, output_find, output_insert, n=None, stream=None, mode=IAF_RACE):
+        _call("b2co_oa_insert_and_find", self._h, _ptr(values), _ptr(output_find), _ptr(output_insert),
+              C.c_uint64(self._n(values, n)), C.c_int(mode), _stream(stream))
+
+    def InsertAndFindAsync(self, values, output_find, output_insert, n=None, stream=None, mode=IAF_RACE):
+        _call("b2co_oa_insert_and_find_async", self._h, _ptr(values), _ptr(output_find), _ptr(output_insert),
+              C.c_uint64(self._n(values, n)), C.c_int(mode), _stream(stream))
+
+    def Erase(self, keys, n=None, stream=None) -> int:
+        f = C.c_uint64()
+        _call("b2co_oa_erase", self._h, _ptr(keys), C.c_uint64(self._n(keys, n)), _stream(stream), C.byref(f))
+        return f.value
+
+    def EraseAsync(self, keys, n=None, stream=None):
+        _call("b2co_oa_erase_async", self._h, _ptr(keys), C.c_uint64(self._n(keys, n)), _stream(stream))
+
+    # -- lookups ----------------------------------------------------------------
+    def Find(self, keys, output_values, n=None, stream=None):
+        _call("b2co_oa_find", self._h, _ptr(keys), _ptr(output_values), C.c_uint64(self._n(keys, n)),
+              _stream(stream))
+
+    def FindAsync(self, keys, output_values, n=None, stream=None):
+        _call("b2co_oa_find_async", self._h, _ptr(keys), _ptr(output_values), C.c_uint64(self._n(keys, n)),
+              _stream(stream))
+
+    def FindIf(self, keys, stencil, output_values, n=None, stream=None):
+        _call("b2co_oa_find_if", self._h, _ptr(keys), _ptr(stencil), _ptr(output_values),
+              C.c_uint64(self._n(keys, n)), _stream(stream))
+
+    def FindIfAsync(self, keys, stencil, output_values, n=None, stream=None):
+        _call("b2co_oa_find_if_async", self._h, _ptr(keys), _ptr(stencil), _ptr(output_values),
+              C.c_uint64(self._n(keys, n)), _stream(stream))
+
+    def Contains(self, keys, output_values, n=None, stream=None):
+        _call("b2co_oa_contains", self._h, _ptr(keys), _ptr(output_values), C.c_uint64(self._n(keys, n)),
+              _stream(stream))
+
+    def ContainsAsync(self, keys, output_values, n=None, stream=None):
+        _call("b2co_oa_contains_async", self._h, _ptr(keys), _ptr(output_values), C.c_uint64(self._n(keys, n)),
+              _stream(stream))
+
+    def ContainsIf(self, keys, stencil, output_values, n=None, stream=None):
+        _call("b2co_oa_contains_if", self._h, _ptr(keys), _ptr(stencil), _ptr(output_values),
+              C.c_uint64(self._n(keys, n)), _stream(stream))
+
+    def ContainsIfAsync(self, keys, stencil, output_values, n=None, stream=None):
+        _call("b2co_oa_contains_if_async", self._h, _ptr(keys), _ptr(stencil), _ptr(output_values),
+              C.c_uint64(self._n(keys, n)), _stream(stream))
+
+    def Count(self, keys, n=None, stream=None) -> int:
+        c = C.c_uint64()
+        _call("b2co_oa_count", self._h, _ptr(keys), C.c_uint64(self._n(keys, n)), _stream(stream), C.byref(c))
+        return c.value
+
+    def FindHost(self, host_keys: np.ndarray, host_out: np.ndarray, stream=None):
+        """Find with host (ideally pinned) buffers; copies overlap the probing."""
+        n = len(host_keys)
+        _call("b2co_oa_find_host", self._h, C.c_void_p(host_keys.ctypes.data), C.c_void_p(host_out.ctypes.data),
+              C.c_uint64(n), _stream(stream))
+
+    def set_find_shape(self, lanes_per_key: int, keys_per_lane: int):
+        _call("b2co_oa_set_find_shape", self._h, C.c_uint32(lanes_per_key), C.c_uint32(keys_per_lane))
+
+    @staticmethod
+    def _n(t, n):
+        if n is not None:
+            return int(n)
+        return 0 if t is None else int(t.shape[0])
+
+
+def _device_bytes(ptr: int, nbytes: int) -> np.ndarray:
+    """Copy `nbytes` of device memory at `ptr` into a host numpy array."""
+    from cuda.bindings import runtime as rt
+    out = np.empty(nbytes, dtype=np.uint8)
+    (err,) = rt.cudaMemcpy(out.ctypes.data, ptr, nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    if err != rt.cudaError_t.cudaSuccess:
+        raise CudaError(f"cudaMemcpy failed ({err})")
+    return out
+
+
+class StaticMap(_OaBase):
+    """StaticMap<Key, T> (include/static_map.h:29-35).  Defaults follow the
+    reference: LinearProbing<murmurhash3_32> with bucket size 5."""
+
+    def __init__(self, capacity, empty_key, empty_value, key_dtype=None, value_dtype=None, bucket_size=5,
+                 probing=PROBE_LINEAR, hash_kind=HASH_MURMUR3_32, erased_key=None, stream=None):
+        import torch
+        super().__init__(capacity, empty_key, empty_value, key_dtype or torch.int32, value_dtype or torch.int32,
+                         bucket_size, probing, hash_kind, erased_key, stream)
+
+    def InsertOrAssign(self, values, n=None, stream=None, with_assigned=False):
+        f, a = C.c_uint64(), C.c_uint64()
+        _call("b2co_oa_insert_or_assign", self._h, _ptr(values), C.c_uint64(self._n(values, n)), _stream(stream),
+              C.byref(f), C.byref(a))
+        return (f.value, a.value) if with_assigned else f.value
+
+    def InsertOrAssignAsync(self, values, n=None, stream=None):
+        _call("b2co_oa_insert_or_assign_async", self._h, _ptr(values), C.c_uint64(self._n(values, n)),
+              _stream(stream))
+
+    def AssignIfAsync(self, values, stencil, n=None, stream=None):
+        _call("b2co_oa_assign_if_async", self._h, _ptr(values), _ptr(stencil), C.c_uint64(self._n(values, n)),
+              _stream(stream))
+
+
+class StaticSet(_OaBase):
+    """StaticSet<Key> (include/static_set.h:27-32).  Defaults follow the
+    reference: DoubleHashing<xxhash_32> with bucket size 5."""
+
+    def __init__(self, capacity, empty_key, key_dtype=None, bucket_size=5, probing=PROBE_DOUBLE,
+                 hash_kind=HASH_XXH32, erased_key=None, stream=None):
+        import torch
+        super().__init__(capacity, empty_key, 0, key_dtype or torch.int32, None, bucket_size, probing, hash_kind,
+                         erased_key, stream)
+
+
+class DynamicMap:
+    """DynamicMap<Key, T> (include/dynamic_map.h:26-29)."""
+
+    kExactDedup, kAppendUnique = INSERT_EXACT_DEDUP, INSERT_APPEND_UNIQUE
+
+    def __init__(self, initial_capacity, empty_key, empty_value, erased_key, key_dtype=None, value_dtype=None,
+                 bucket_size=5, probing=PROBE_LINEAR, hash_kind=HASH_MURMUR3_32, stream=None):
+        import torch
+        key_dtype = key_dtype or torch.int32
+        value_dtype = value_dtype or torch.int32
+        kb, vb = _dtype_bytes(key_dtype), _dtype_bytes(value_dtype)
+        self.key_bytes, self.value_bytes = kb, vb
+        d = OaDesc(kb, vb, bucket_size, probing, hash_kind, 0, _bits(empty_key, kb), _bits(empty_value, vb),
+                   _bits(erased_key, kb))
+        h = C.c_void_p()
+        _call("b2co_dmap_create", C.byref(d), C.c_uint64(initial_capacity), _stream(stream), C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_dmap_destroy(h)
+            self._h = None
+
+    def _u64(self, name):
+        v = C.c_uint64()
+        _call(name, self._h, C.byref(v))
+        return v.value
+
+    def Size(self):
+        return self._u64("b2co_dmap_size")
+
+    def Capacity(self):
+        return self._u64("b2co_dmap_capacity")
+
+    def NumSubmaps(self):
+        return self._u64("b2co_dmap_num_submaps")
+
+    def Reserve(self, n, stream=None):
+        _call("b2co_dmap_reserve", self._h, C.c_uint64(n), _stream(stream))
+
+    def Insert(self, values, n=None, stream=None, mode=INSERT_EXACT_DEDUP) -> int:
+        v = C.c_uint64()
+        _call("b2co_dmap_insert", self._h, _ptr(values), C.c_uint64(_OaBase._n(values, n)), C.c_int(mode),
+              _stream(stream), C.byref(v))
+        return v.value
+
+    def InsertOrAssign(self, values, n=None, stream=None) -> int:
+        v = C.c_uint64()
+        _call("b2co_dmap_insert_or_assign", self._h, _ptr(values), C.c_uint64(_OaBase._n(values, n)),
+              _stream(stream), C.byref(v))
+        return v.value
+
+    def Find(self, keys, output_values, n=None, stream=None):
+        _call("b2co_dmap_find", self._h, _ptr(keys), _ptr(output_values), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def Contains(self, keys, output_values, n=None, stream=None):
+        _call("b2co_dmap_contains", self._h, _ptr(keys), _ptr(output_values), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def Erase(self, keys, n=None, stream=None) -> int:
+        v = C.c_uint64()
+        _call("b2co_dmap_erase", self._h, _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream),
+              C.byref(v))
+        return v.value
+
+    def Clear(self, stream=None):
+        _call("b2co_dmap_clear", self._h, _stream(stream))
+
+
+class BloomFilter:
+    """BloomFilter<Key> with the default policy (include/bloom_filter.h:37-39)."""
+
+    def __init__(self, num_blocks, key_dtype=None, seed=0, stream=None):
+        import torch
+        key_dtype = key_dtype or torch.uint64
+        self.key_bytes = _dtype_bytes(key_dtype)
+        h = C.c_void_p()
+        _call("b2co_bloom_create", C.c_uint64(num_blocks), C.c_uint32(self.key_bytes), C.c_uint64(seed),
+              _stream(stream), C.byref(h))
+        self._h = h
+        self.num_blocks = num_blocks
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_bloom_destroy(h)
+            self._h = None
+
+    def Data(self) -> int:
+        p = C.c_void_p()
+        _call("b2co_bloom_data", self._h, C.byref(p))
+        return p.value
+
+    def words(self) -> np.ndarray:
+        """The filter's words copied to the host (uint32, 8 per block)."""
+        return _device_bytes(self.Data(), self.num_blocks * 32).view(np.uint32)
+
+    def Clear(self, stream=None):
+        _call("b2co_bloom_clear", self._h, _stream(stream))
+
+    def ClearAsync(self, stream=None):
+        _call("b2co_bloom_clear_async", self._h, _stream(stream))
+
+    def Add(self, keys, n=None, stream=None):
+        _call("b2co_bloom_add", self._h, _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def AddAsync(self, keys, n=None, stream=None):
+        _call("b2co_bloom_add_async", self._h, _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def AddIf(self, keys, stencil, n=None, stream=None):
+        _call("b2co_bloom_add_if", self._h, _ptr(keys), _ptr(stencil), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def Contains(self, keys, output_values, n=None, stream=None):
+        _call("b2co_bloom_contains", self._h, _ptr(keys), _ptr(output_values), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def ContainsAsync(self, keys, output_values, n=None, stream=None):
+        _call("b2co_bloom_contains_async", self._h, _ptr(keys), _ptr(output_values),
+              C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def ContainsIf(self, keys, stencil, output_values, n=None, stream=None):
+        _call("b2co_bloom_contains_if", self._h, _ptr(keys), _ptr(stencil), _ptr(output_values),
+              C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def Merge(self, other, stream=None):
+        _call("b2co_bloom_merge", self._h, other._h, _stream(stream))
+
+    def MergeAsync(self, other, stream=None):
+        _call("b2co_bloom_merge_async", self._h, other._h, _stream(stream))
+
+    def Intersect(self, other, stream=None):
+        _call("b2co_bloom_intersect", self._h, other._h, _stream(stream))
+
+
+class HyperLogLog:
+    """HyperLogLog<Key> for int32/int64 keys (include/hyperloglog.h:23-59)."""
+
+    def __init__(self, precision, key_dtype=None, stream=None):
+        import torch
+        key_dtype = key_dtype or torch.int64
+        self.key_bytes = _dtype_bytes(key_dtype)
+        h = C.c_void_p()
+        _call("b2co_hll_create", C.c_uint32(precision), C.c_uint32(self.key_bytes), _stream(stream), C.byref(h))
+        self._h = h
+        self.precision = precision
+
+    @classmethod
+    def CreateWithSketchSizeKB(cls, kb, key_dtype=None, stream=None):
+        p = C.c_uint32()
+        _call("b2co_hll_precision_for_sketch_kb", C.c_uint32(kb), C.byref(p))
+        return cls(p.value, key_dtype, stream)
+
+    @classmethod
+    def CreateWithPrecision(cls, precision, key_dtype=None, stream=None):
+        return cls(precision, key_dtype, stream)
+
+    @classmethod
+    def CreateWithStandardDeviation(cls, deviation, key_dtype=None, stream=None):
+        p = C.c_uint32()
+        _call("b2co_hll_precision_for_deviation", C.c_double(deviation), C.byref(p))
+        return cls(p.value, key_dtype, stream)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_hll_destroy(h)
+            self._h = None
+
+    def SketchSizeKB(self):
+        return (1 << self.precision) // 1024
+
+    def Data(self) -> int:
+        p = C.c_void_p()
+        _call("b2co_hll_data", self._h, C.byref(p))
+        return p.value
+
+    def registers(self) -> np.ndarray:
+        """The 2^precision register bytes copied to the host."""
+        return _device_bytes(self.Data(), 1 << self.precision)
+
+    def Clear(self, stream=None):
+        _call("b2co_hll_clear", self._h, _stream(stream))
+
+    def Add(self, keys, n=None, stream=None):
+        _call("b2co_hll_add", self._h, _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def AddAsync(self, keys, n=None, stream=None):
+        _call("b2co_hll_add_async", self._h, _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def Merge(self, other, stream=None):
+        _call("b2co_hll_merge", self._h, other._h, _stream(stream))
+
+    def Estimate(self, stream=None) -> int:
+        v = C.c_uint64()
+        _call("b2co_hll_estimate", self._h, _stream(stream), C.byref(v))
+        return v.value
+
+    def Histogram(self, stream=None) -> np.ndarray:
+        h = np.zeros(65, dtype=np.uint32)
+        _call("b2co_hll_histogram", self._h, _stream(stream), C.c_void_p(h.ctypes.data))
+        return h
+
+
+def hll_finalize(precision: int, hist) -> int:
+    hist = np.ascontiguousarray(hist, dtype=np.uint32)
+    v = C.c_uint64()
+    _call("b2co_hll_finalize", C.c_uint32(precision), C.c_void_p(hist.ctypes.data), C.byref(v))
+    return v.value
+
+
+def hll_bias_data(precision: int):
+    raw, bias = C.POINTER(C.c_double)(), C.POINTER(C.c_double)()
+    n, thr = C.c_uint32(), C.c_double()
+    _call("b2co_hll_bias_data", C.c_uint32(precision), C.byref(raw), C.byref(bias), C.byref(n), C.byref(thr))
+    return (np.ctypeslib.as_array(raw, shape=(n.value,)).copy(), np.ctypeslib.as_array(bias, shape=(n.value,)).copy(),
+            thr.value)

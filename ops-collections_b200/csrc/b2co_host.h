@@ -1,0 +1,65 @@
+// b2co_host.h -- host-side internals shared by the library's translation units:
+// error reporting, launch geometry and the per-slot-layout launcher tables.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/b2co.h"
+#include "b2co_common.cuh"
+
+namespace b2co {
+
+// Records `msg` as this thread's last error and returns `status`.
+int fail(int status, std::string const& msg);
+// Maps a CUDA error to B2CO_ECUDA with the failing call's name.
+int cuda_fail(cudaError_t e, char const* what);
+inline int ok() { return B2CO_OK; }
+
+#define B2CO_CUDA(call)                                    \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return ::b2co::cuda_fail(e_, #call); \
+    } while (0)
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+// Grid for a grid-stride kernel: enough blocks for `work` items at `per_block`
+// items per block, capped at the blocks that can be resident at once.
+uint32_t grid_for(void const* kernel, uint32_t block, uint64_t work, uint64_t per_block);
+
+// Largest batch a single launch accepts: 32-bit indices plus one grid stride
+// must not overflow (the reference's CheckedBatchSize,
+// detail/open_addressing/open_addressing_impl.h:534-545).
+constexpr uint64_t kMaxBatch = (1ull << 32) - (1ull << 22);
+
+// Capacity prime rule (include/utility/prime.h:15 regenerated; see capacity.cpp).
+uint64_t prime_at_least(uint64_t n);
+uint64_t prime_table_last();
+
+struct OaArgs;
+
+// Launchers for one slot layout; B (bucket size) is dispatched at run time.
+struct OaOps {
+    int (*clear)(OaArgs const& a, cudaStream_t s);
+    int (*insert)(OaArgs const& a, uint32_t b, void const* pairs, uint8_t const* stencil, uint32_t n, bool assign,
+                  unsigned long long* counters, cudaStream_t s);
+    int (*assign_if)(OaArgs const& a, uint32_t b, void const* pairs, uint8_t const* stencil, uint32_t n,
+                     cudaStream_t s);
+    int (*iaf_race)(OaArgs const& a, uint32_t b, void const* pairs, void* found, uint8_t* inserted, uint32_t n,
+                    cudaStream_t s);
+    int (*iaf_first)(OaArgs const& a, uint32_t b, void const* pairs, void* found, uint8_t* inserted, uint32_t n,
+                     uint32_t* pos, uint32_t* newbits, uint32_t* owner, cudaStream_t s);
+    int (*find)(OaArgs const& a, uint32_t b, uint32_t lanes, uint32_t items, bool contains, void const* keys,
+                uint8_t const* stencil, void* out, uint32_t n, cudaStream_t s);
+    int (*erase)(OaArgs const& a, uint32_t b, void const* keys, uint32_t n, unsigned long long* counters,
+                 cudaStream_t s);
+    int (*count)(OaArgs const& a, uint32_t b, void const* keys, uint32_t n, unsigned long long* counter,
+                 cudaStream_t s);
+};
+
+extern OaOps const kOpsSet4, kOpsSet8, kOpsMap44, kOpsMap48, kOpsMap84, kOpsMap88;
+
+}  // namespace b2co

@@ -1,0 +1,326 @@
+// bloom.cu -- BloomFilter<Key> with the reference's default policy
+// (bloom_filter_policy.h:54-181): 256-bit blocks of 8 uint32 words, xxh64 of
+// the key, block = mulhi32(upper hash, numBlocks), one bit per word at
+// (salt[w] * lower hash) >> 27.
+//
+// B200 design: a block is exactly one 32-byte L2 sector.  Add issues the
+// block's 8 word bits as four 64-bit atomic ORs that need no return value
+// (RED), all to that one sector; lanes of a warp that hit the same block are
+// merged first (match_any) so each distinct block takes one set of REDs.
+// Contains reads the sector with two 16-byte loads.  Merge/Intersect stream
+// 16 bytes per lane.
+#include <new>
+
+#include "b2co_host.h"
+
+using namespace b2co;
+
+namespace {
+
+// Split-block Bloom filter salts of the Parquet specification; the reference's
+// salt table starts with these eight (bloom_filter_policy.h:170-178).
+__constant__ uint32_t kSalts[8] = {0x47b6137bu, 0x44974d91u, 0x8824ad5bu, 0xa2b7289du,
+                                   0x705495c7u, 0x2df1424bu, 0x9efc4947u, 0x5c6bfb31u};
+
+template <int KB>
+__device__ __forceinline__ void locate(uint64_t key, uint64_t seed, uint32_t nblocks, uint32_t& block, uint32_t& lower)
+{
+    uint64_t h = xxh64<KB>(key, seed);
+    block = uint32_t((uint64_t(uint32_t(h >> 32)) * nblocks) >> 32);
+    lower = uint32_t(h);
+}
+
+__device__ __forceinline__ uint32_t word_bit(int w, uint32_t lower) { return 1u << ((kSalts[w] * lower) >> 27); }
+
+template <int KB>
+__device__ __forceinline__ uint64_t load_key(void const* keys, uint64_t i)
+{
+    if constexpr (KB == 8) return __ldg(reinterpret_cast<unsigned long long const*>(keys) + i);
+    else return __ldg(reinterpret_cast<uint32_t const*>(keys) + i);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(256) k_bloom_add(uint32_t* words, uint32_t nblocks, uint64_t seed, void const* keys,
+                                                   uint8_t const* stencil, uint64_t n)
+{
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        uint64_t i = base + (threadIdx.x & 31);
+        bool live = i < n && (!stencil || stencil[i]);
+        uint32_t block = 0xffffffffu, lower = 0;
+        if (live) locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower);
+        uint32_t pat[8];
+#pragma unroll
+        for (int w = 0; w < 8; ++w) pat[w] = live ? word_bit(w, lower) : 0u;
+        // lanes sharing a block OR their patterns together; the lowest lane issues the REDs
+        uint32_t peers = __match_any_sync(0xffffffffu, block);
+        uint32_t const lane = threadIdx.x & 31;
+        if (__popc(peers) > 1) {
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                uint32_t acc = pat[w];
+                for (uint32_t m = peers; m; m &= m - 1) acc |= __shfl_sync(peers, pat[w], __ffs(m) - 1);
+                pat[w] = acc;
+            }
+        }
+        if (live && lane == uint32_t(__ffs(peers) - 1)) {
+            unsigned long long* p = reinterpret_cast<unsigned long long*>(words + uint64_t(block) * 8);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) atomicOr(p + q, (unsigned long long)pat[2 * q] | ((unsigned long long)pat[2 * q + 1] << 32));
+        }
+    }
+}
+
+template <int KB>
+__global__ void __launch_bounds__(256) k_bloom_contains(uint32_t const* words, uint32_t nblocks, uint64_t seed,
+                                                        void const* keys, uint8_t const* stencil, uint8_t* out,
+                                                        uint64_t n)
+{
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint8_t r = 0;
+        if (!stencil || stencil[i]) {
+            uint32_t block, lower;
+            locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower);
+            uint4 const* p = reinterpret_cast<uint4 const*>(words + uint64_t(block) * 8);
+            uint4 a = __ldg(p), b = __ldg(p + 1);
+            uint32_t const w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+            bool all = true;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                uint32_t bit = word_bit(j, lower);
+                all &= (w[j] & bit) == bit;
+            }
+            r = all;
+        }
+        out[i] = r;
+    }
+}
+
+template <int OP>  // 0 = or, 1 = and
+__global__ void __launch_bounds__(256) k_bloom_combine(uint4* dst, uint4 const* src, uint64_t n16)
+{
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n16; i += stride) {
+        uint4 a = dst[i], b = __ldg(src + i);
+        if (OP == 0) a = make_uint4(a.x | b.x, a.y | b.y, a.z | b.z, a.w | b.w);
+        else a = make_uint4(a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w);
+        dst[i] = a;
+    }
+}
+
+cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+struct b2co_bloom {
+    uint32_t* words = nullptr;
+    uint64_t num_blocks = 0;
+    uint32_t key_bytes = 0;
+    uint64_t seed = 0;
+};
+
+namespace {
+
+int check(b2co_bloom const* f)
+{
+    if (!f || !f->words) return fail(B2CO_ELOGIC, "BloomFilter: a moved-from filter cannot participate");
+    return B2CO_OK;
+}
+
+// ValidateCompatible (bloom_filter_query.inl:197-215).
+int check_pair(b2co_bloom const* a, b2co_bloom const* b, char const* op)
+{
+    if (int st = check(a)) return st;
+    if (int st = check(b)) return st;
+    if (a->num_blocks != b->num_blocks)
+        return fail(B2CO_EINVAL, std::string("BloomFilter::") + op + ": filters have different block extents");
+    if (a->seed != b->seed || a->key_bytes != b->key_bytes)
+        return fail(B2CO_EINVAL, std::string("BloomFilter::") + op + ": filters have different policies");
+    return B2CO_OK;
+}
+
+int add_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_stencil, uint64_t n, cudaStream_t s)
+{
+    if (int st = check(f)) return st;
+    if (n == 0) return B2CO_OK;
+    if (!keys) return fail(B2CO_EINVAL, "BloomFilter::Add: keys must not be null when keyNum is non-zero");
+    if (use_stencil && !stencil)
+        return fail(B2CO_EINVAL, "BloomFilter::AddIf: stencil must not be null when keyNum is non-zero");
+    void (*k)(uint32_t*, uint32_t, uint64_t, void const*, uint8_t const*, uint64_t) =
+        f->key_bytes == 8 ? k_bloom_add<8> : k_bloom_add<4>;
+    k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks), f->seed, keys, stencil,
+                                                           n);
+    B2CO_CUDA(cudaGetLastError());
+    return B2CO_OK;
+}
+
+int contains_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_stencil, uint8_t* out, uint64_t n,
+                  cudaStream_t s)
+{
+    if (int st = check(f)) return st;
+    if (n == 0) return B2CO_OK;
+    if (!keys) return fail(B2CO_EINVAL, "BloomFilter::Contains: keys must not be null when keyNum is non-zero");
+    if (!out) return fail(B2CO_EINVAL, "BloomFilter::Contains: outputValues must not be null when keyNum is non-zero");
+    if (use_stencil && !stencil)
+        return fail(B2CO_EINVAL, "BloomFilter::ContainsIf: stencil must not be null when keyNum is non-zero");
+    void (*k)(uint32_t const*, uint32_t, uint64_t, void const*, uint8_t const*, uint8_t*, uint64_t) =
+        f->key_bytes == 8 ? k_bloom_contains<8> : k_bloom_contains<4>;
+    k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks), f->seed, keys, stencil,
+                                                           out, n);
+    B2CO_CUDA(cudaGetLastError());
+    return B2CO_OK;
+}
+
+template <int OP>
+int combine(b2co_bloom* f, b2co_bloom const* o, cudaStream_t s, char const* name)
+{
+    if (int st = check_pair(f, o, name)) return st;
+    if (f == o) return B2CO_OK;
+    uint64_t n16 = f->num_blocks * 2;
+    auto k = k_bloom_combine<OP>;
+    k<<<grid_for((void const*)k, 256, n16, 256), 256, 0, s>>>(reinterpret_cast<uint4*>(f->words),
+                                                              reinterpret_cast<uint4 const*>(o->words), n16);
+    B2CO_CUDA(cudaGetLastError());
+    return B2CO_OK;
+}
+
+int sync(cudaStream_t s)
+{
+    B2CO_CUDA(cudaStreamSynchronize(s));
+    return B2CO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b2co_bloom_create(uint64_t num_blocks, uint32_t key_bytes, uint64_t seed, b2co_stream stream, b2co_bloom** out)
+{
+    if (!out) return fail(B2CO_EINVAL, "null output");
+    *out = nullptr;
+    if (num_blocks == 0) return fail(B2CO_EINVAL, "BloomFilter: numBlocks must be greater than zero");
+    if (num_blocks > 0xffffffffull)
+        return fail(B2CO_ERANGE, "BloomFilter: numBlocks exceeds the supported block-index range");
+    if (key_bytes != 4 && key_bytes != 8) return fail(B2CO_EINVAL, "BloomFilter: key_bytes must be 4 or 8");
+    auto* f = new (std::nothrow) b2co_bloom;
+    if (!f) return fail(B2CO_ENOMEM, "host allocation failed");
+    f->num_blocks = num_blocks;
+    f->key_bytes = key_bytes;
+    f->seed = seed;
+    cudaError_t e = cudaMalloc(&f->words, num_blocks * 32);
+    if (e != cudaSuccess) {
+        delete f;
+        return cuda_fail(e, "BloomFilter allocation");
+    }
+    if (int st = b2co_bloom_clear(f, stream)) {
+        b2co_bloom_destroy(f);
+        return st;
+    }
+    *out = f;
+    return B2CO_OK;
+}
+
+int b2co_bloom_destroy(b2co_bloom* f)
+{
+    if (!f) return B2CO_OK;
+    if (f->words) cudaFree(f->words);
+    delete f;
+    return B2CO_OK;
+}
+
+int b2co_bloom_data(b2co_bloom const* f, uint32_t** words)
+{
+    if (int st = check(f)) return st;
+    if (!words) return fail(B2CO_EINVAL, "null output");
+    *words = f->words;
+    return B2CO_OK;
+}
+
+int b2co_bloom_num_blocks(b2co_bloom const* f, uint64_t* nb)
+{
+    if (int st = check(f)) return st;
+    if (!nb) return fail(B2CO_EINVAL, "null output");
+    *nb = f->num_blocks;
+    return B2CO_OK;
+}
+
+int b2co_bloom_clear_async(b2co_bloom* f, b2co_stream s)
+{
+    if (int st = check(f)) return st;
+    B2CO_CUDA(cudaMemsetAsync(f->words, 0, f->num_blocks * 32, cs(s)));
+    return B2CO_OK;
+}
+
+int b2co_bloom_clear(b2co_bloom* f, b2co_stream s)
+{
+    if (int st = b2co_bloom_clear_async(f, s)) return st;
+    return sync(cs(s));
+}
+
+int b2co_bloom_add_async(b2co_bloom* f, void const* keys, uint64_t n, b2co_stream s)
+{
+    return add_impl(f, keys, nullptr, false, n, cs(s));
+}
+
+int b2co_bloom_add(b2co_bloom* f, void const* keys, uint64_t n, b2co_stream s)
+{
+    if (int st = add_impl(f, keys, nullptr, false, n, cs(s))) return st;
+    return sync(cs(s));
+}
+
+int b2co_bloom_add_if_async(b2co_bloom* f, void const* keys, uint8_t const* stencil, uint64_t n, b2co_stream s)
+{
+    return add_impl(f, keys, stencil, true, n, cs(s));
+}
+
+int b2co_bloom_add_if(b2co_bloom* f, void const* keys, uint8_t const* stencil, uint64_t n, b2co_stream s)
+{
+    if (int st = add_impl(f, keys, stencil, true, n, cs(s))) return st;
+    return sync(cs(s));
+}
+
+int b2co_bloom_contains_async(b2co_bloom* f, void const* keys, uint8_t* out, uint64_t n, b2co_stream s)
+{
+    return contains_impl(f, keys, nullptr, false, out, n, cs(s));
+}
+
+int b2co_bloom_contains(b2co_bloom* f, void const* keys, uint8_t* out, uint64_t n, b2co_stream s)
+{
+    if (int st = contains_impl(f, keys, nullptr, false, out, n, cs(s))) return st;
+    return sync(cs(s));
+}
+
+int b2co_bloom_contains_if_async(b2co_bloom* f, void const* keys, uint8_t const* stencil, uint8_t* out, uint64_t n,
+                                 b2co_stream s)
+{
+    return contains_impl(f, keys, stencil, true, out, n, cs(s));
+}
+
+int b2co_bloom_contains_if(b2co_bloom* f, void const* keys, uint8_t const* stencil, uint8_t* out, uint64_t n,
+                           b2co_stream s)
+{
+    if (int st = contains_impl(f, keys, stencil, true, out, n, cs(s))) return st;
+    return sync(cs(s));
+}
+
+int b2co_bloom_merge_async(b2co_bloom* f, b2co_bloom const* o, b2co_stream s) { return combine<0>(f, o, cs(s), "Merge"); }
+
+int b2co_bloom_merge(b2co_bloom* f, b2co_bloom const* o, b2co_stream s)
+{
+    if (int st = combine<0>(f, o, cs(s), "Merge")) return st;
+    return sync(cs(s));
+}
+
+int b2co_bloom_intersect_async(b2co_bloom* f, b2co_bloom const* o, b2co_stream s)
+{
+    return combine<1>(f, o, cs(s), "Intersect");
+}
+
+int b2co_bloom_intersect(b2co_bloom* f, b2co_bloom const* o, b2co_stream s)
+{
+    if (int st = combine<1>(f, o, cs(s), "Intersect")) return st;
+    return sync(cs(s));
+}
+
+}  // extern "C"

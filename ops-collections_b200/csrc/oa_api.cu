@@ -1,0 +1,491 @@
+// oa_api.cu -- C ABI of the open-addressing containers (StaticMap/StaticSet).
+//
+// Host conventions follow detail/open_addressing/open_addressing_impl.h: zero
+// items is a no-op, a NULL input makes a sync insert report every item failed
+// and an async call return, batches beyond the kernel index range are a
+// length error, sync calls synchronize the stream and read the counters back.
+#include <cstring>
+#include <new>
+
+#include "b2co_host.h"
+#include "oa_kernels.cuh"
+
+using namespace b2co;
+
+struct b2co_oa_table {
+    b2co_oa_desc desc{};
+    OaArgs args{};
+    OaOps const* ops = nullptr;
+    uint64_t capacity = 0;
+    int device = 0;
+    unsigned long long* d_counters = nullptr;  // [failed, assigned]
+    unsigned long long* h_counters = nullptr;  // pinned mirror
+    // first-wins InsertAndFind scratch, grown on demand
+    uint32_t* d_pos = nullptr;
+    uint64_t pos_cap = 0;
+    uint32_t* d_newbits = nullptr;
+    uint32_t* d_owner = nullptr;
+    // host-buffer Find pipeline
+    void* stage = nullptr;
+    uint64_t stage_keys = 0;
+    cudaStream_t pipe[2] = {nullptr, nullptr};
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    uint32_t find_lanes = 0, find_items = 0;
+};
+
+namespace {
+
+uint64_t mask_bytes(uint64_t v, uint32_t n) { return n >= 8 ? v : (v & ((1ull << (8 * n)) - 1ull)); }
+
+OaOps const* ops_for(uint32_t kb, uint32_t vb)
+{
+    if (kb == 4 && vb == 0) return &kOpsSet4;
+    if (kb == 8 && vb == 0) return &kOpsSet8;
+    if (kb == 4 && vb == 4) return &kOpsMap44;
+    if (kb == 4 && vb == 8) return &kOpsMap48;
+    if (kb == 8 && vb == 4) return &kOpsMap84;
+    if (kb == 8 && vb == 8) return &kOpsMap88;
+    return nullptr;
+}
+
+uint32_t slot_bytes(uint32_t kb, uint32_t vb)
+{
+    if (vb == 0) return kb;
+    return (kb == 4 && vb == 4) ? 8 : 16;
+}
+
+int check_table(b2co_oa_table const* t)
+{
+    if (!t || !t->args.slots) return fail(B2CO_ELOGIC, "table is null or has no storage");
+    return B2CO_OK;
+}
+
+int check_batch(uint64_t n)
+{
+    if (n > kMaxBatch) return fail(B2CO_ERANGE, "OpenAddressing: batch size exceeds the kernel index range");
+    return B2CO_OK;
+}
+
+cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Default lookup shape per layout; the autotuner overrides it per table.
+void default_shape(b2co_oa_table* t)
+{
+    uint32_t sb = slot_bytes(t->desc.key_bytes, t->desc.value_bytes);
+    if (t->desc.bucket_size == 1) {
+        t->find_lanes = 1;
+        t->find_items = 4;
+    } else if (sb == 16) {
+        t->find_lanes = 1;
+        t->find_items = 2;
+    } else {
+        t->find_lanes = 1;
+        t->find_items = 2;
+    }
+}
+
+int launch_find(b2co_oa_table* t, bool contains, void const* keys, uint8_t const* stencil, void* out, uint64_t n,
+                cudaStream_t s)
+{
+    return t->ops->find(t->args, t->desc.bucket_size, t->find_lanes, t->find_items, contains, keys, stencil, out,
+                        uint32_t(n), s);
+}
+
+int sync_counters(b2co_oa_table* t, cudaStream_t s, int words)
+{
+    B2CO_CUDA(cudaMemcpyAsync(t->h_counters, t->d_counters, sizeof(unsigned long long) * words,
+                              cudaMemcpyDeviceToHost, s));
+    B2CO_CUDA(cudaStreamSynchronize(s));
+    return B2CO_OK;
+}
+
+int ensure_first_wins_scratch(b2co_oa_table* t, uint64_t n)
+{
+    if (!t->d_newbits) {
+        uint64_t words = (t->capacity + 31) / 32;
+        B2CO_CUDA(cudaMalloc(&t->d_newbits, words * 4));
+        B2CO_CUDA(cudaMalloc(&t->d_owner, t->capacity * 4));
+    }
+    if (t->pos_cap < n) {
+        if (t->d_pos) cudaFree(t->d_pos);
+        t->d_pos = nullptr;
+        t->pos_cap = 0;
+        B2CO_CUDA(cudaMalloc(&t->d_pos, n * 4));
+        t->pos_cap = n;
+    }
+    return B2CO_OK;
+}
+
+}  // namespace
+
+// Table creation with the clear optional: DynamicMap prepares its next submap
+// uncleared and clears it on a side stream (the reference's DeferredClear
+// constructor, include/static_map.h:611).
+int b2co_oa_create_ex(b2co_oa_desc const* d, uint64_t requested, bool clear, b2co_stream stream,
+                      b2co_oa_table** out)
+{
+    if (!d || !out) return fail(B2CO_EINVAL, "null descriptor or output");
+    *out = nullptr;
+    if (d->key_bytes != 4 && d->key_bytes != 8) return fail(B2CO_EINVAL, "key_bytes must be 4 or 8");
+    if (d->value_bytes != 0 && d->value_bytes != 4 && d->value_bytes != 8)
+        return fail(B2CO_EINVAL, "value_bytes must be 0, 4 or 8");
+    if (d->probing > B2CO_PROBE_DOUBLE) return fail(B2CO_EINVAL, "unknown probing scheme");
+    if (d->hash > B2CO_HASH_XXH64) return fail(B2CO_EINVAL, "unknown hash");
+    if (d->reserved != 0) return fail(B2CO_EINVAL, "reserved descriptor field must be 0");
+    uint64_t cap = 0;
+    int st = b2co_oa_valid_capacity(requested, d->bucket_size, d->probing, &cap);
+    if (st) return st;
+    if (cap > 0xffffffffull)
+        return fail(B2CO_ERANGE, "capacity exceeds the 32-bit slot index of the kernels");
+
+    auto* t = new (std::nothrow) b2co_oa_table;
+    if (!t) return fail(B2CO_ENOMEM, "host allocation failed");
+    t->desc = *d;
+    t->desc.empty_key_bits = mask_bytes(d->empty_key_bits, d->key_bytes);
+    t->desc.erased_key_bits = mask_bytes(d->erased_key_bits, d->key_bytes);
+    t->desc.empty_value_bits = mask_bytes(d->empty_value_bits, d->value_bytes ? d->value_bytes : 8);
+    t->ops = ops_for(d->key_bytes, d->value_bytes);
+    t->capacity = cap;
+    cudaGetDevice(&t->device);
+    default_shape(t);
+
+    uint32_t nb = uint32_t(cap / d->bucket_size);
+    ProbeParams& p = t->args.probe;
+    p.capacity = uint32_t(cap);
+    p.nbuckets = nb;
+    p.mod_nb = make_fastmod(nb);
+    p.mod_nbm1 = make_fastmod(nb > 1 ? nb - 1 : 1);
+    p.probing = d->probing;
+    p.hash = d->hash;
+    t->args.empty_key = t->desc.empty_key_bits;
+    t->args.empty_value = d->value_bytes ? t->desc.empty_value_bits : 0;
+    t->args.erased_key = t->desc.erased_key_bits;
+
+    cudaError_t e = cudaMalloc(&t->args.slots, cap * slot_bytes(d->key_bytes, d->value_bytes));
+    if (e == cudaSuccess) e = cudaMalloc(&t->d_counters, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&t->h_counters, 2 * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        b2co_oa_destroy(t);
+        return cuda_fail(e, "table allocation");
+    }
+    if (clear && (st = b2co_oa_clear(t, stream))) {
+        b2co_oa_destroy(t);
+        return st;
+    }
+    *out = t;
+    return B2CO_OK;
+}
+
+extern "C" {
+
+int b2co_oa_create(b2co_oa_desc const* d, uint64_t requested, b2co_stream stream, b2co_oa_table** out)
+{
+    return b2co_oa_create_ex(d, requested, true, stream, out);
+}
+
+int b2co_oa_destroy(b2co_oa_table* t)
+{
+    if (!t) return B2CO_OK;
+    if (t->args.slots) cudaFree(t->args.slots);
+    if (t->d_counters) cudaFree(t->d_counters);
+    if (t->h_counters) cudaFreeHost(t->h_counters);
+    if (t->d_pos) cudaFree(t->d_pos);
+    if (t->d_newbits) cudaFree(t->d_newbits);
+    if (t->d_owner) cudaFree(t->d_owner);
+    if (t->stage) cudaFree(t->stage);
+    for (auto& s : t->pipe)
+        if (s) cudaStreamDestroy(s);
+    for (auto& e : t->ev)
+        if (e) cudaEventDestroy(e);
+    delete t;
+    return B2CO_OK;
+}
+
+int b2co_oa_capacity(b2co_oa_table const* t, uint64_t* c)
+{
+    if (int st = check_table(t)) return st;
+    if (!c) return fail(B2CO_EINVAL, "null output");
+    *c = t->capacity;
+    return B2CO_OK;
+}
+
+int b2co_oa_data(b2co_oa_table const* t, void** slots)
+{
+    if (int st = check_table(t)) return st;
+    if (!slots) return fail(B2CO_EINVAL, "null output");
+    *slots = t->args.slots;
+    return B2CO_OK;
+}
+
+int b2co_oa_set_erased_key(b2co_oa_table* t, uint64_t erased, b2co_stream)
+{
+    if (int st = check_table(t)) return st;
+    t->desc.erased_key_bits = mask_bytes(erased, t->desc.key_bytes);
+    t->args.erased_key = t->desc.erased_key_bits;
+    return B2CO_OK;
+}
+
+int b2co_oa_clear_async(b2co_oa_table* t, b2co_stream s)
+{
+    if (int st = check_table(t)) return st;
+    return t->ops->clear(t->args, cs(s));
+}
+
+int b2co_oa_clear(b2co_oa_table* t, b2co_stream s)
+{
+    if (int st = b2co_oa_clear_async(t, s)) return st;
+    B2CO_CUDA(cudaStreamSynchronize(cs(s)));
+    return B2CO_OK;
+}
+
+// ---- inserts ---------------------------------------------------------------
+
+static int insert_impl(b2co_oa_table* t, void const* pairs, uint8_t const* stencil, bool use_stencil, uint64_t n,
+                       bool assign, b2co_stream s, uint64_t* failed, uint64_t* assigned)
+{
+    bool sync = failed != nullptr || assigned != nullptr;
+    if (failed) *failed = 0;
+    if (assigned) *assigned = 0;
+    if (int st = check_table(t)) return st;
+    if (n == 0) return B2CO_OK;
+    if (!pairs || (use_stencil && !stencil)) {
+        if (failed) *failed = n;
+        return B2CO_OK;
+    }
+    if (int st = check_batch(n)) return st;
+    cudaStream_t c = cs(s);
+    if (sync) B2CO_CUDA(cudaMemsetAsync(t->d_counters, 0, 2 * sizeof(unsigned long long), c));
+    int st = t->ops->insert(t->args, t->desc.bucket_size, pairs, stencil, uint32_t(n), assign,
+                            sync ? t->d_counters : nullptr, c);
+    if (st || !sync) return st;
+    if ((st = sync_counters(t, c, 2))) return st;
+    if (failed) *failed = t->h_counters[0];
+    if (assigned) *assigned = t->h_counters[1];
+    return B2CO_OK;
+}
+
+int b2co_oa_insert(b2co_oa_table* t, void const* pairs, uint64_t n, b2co_stream s, uint64_t* failed)
+{
+    uint64_t dummy;
+    return insert_impl(t, pairs, nullptr, false, n, false, s, failed ? failed : &dummy, nullptr);
+}
+
+int b2co_oa_insert_async(b2co_oa_table* t, void const* pairs, uint64_t n, b2co_stream s)
+{
+    return insert_impl(t, pairs, nullptr, false, n, false, s, nullptr, nullptr);
+}
+
+int b2co_oa_insert_if(b2co_oa_table* t, void const* pairs, uint8_t const* stencil, uint64_t n, b2co_stream s,
+                      uint64_t* failed)
+{
+    uint64_t dummy;
+    return insert_impl(t, pairs, stencil, true, n, false, s, failed ? failed : &dummy, nullptr);
+}
+
+int b2co_oa_insert_if_async(b2co_oa_table* t, void const* pairs, uint8_t const* stencil, uint64_t n, b2co_stream s)
+{
+    return insert_impl(t, pairs, stencil, true, n, false, s, nullptr, nullptr);
+}
+
+int b2co_oa_insert_or_assign(b2co_oa_table* t, void const* pairs, uint64_t n, b2co_stream s, uint64_t* failed,
+                             uint64_t* assigned)
+{
+    uint64_t f, a;
+    if (t && t->desc.value_bytes == 0) return fail(B2CO_EINVAL, "InsertOrAssign needs a map (value_bytes > 0)");
+    return insert_impl(t, pairs, nullptr, false, n, true, s, failed ? failed : &f, assigned ? assigned : &a);
+}
+
+int b2co_oa_insert_or_assign_async(b2co_oa_table* t, void const* pairs, uint64_t n, b2co_stream s)
+{
+    if (t && t->desc.value_bytes == 0) return fail(B2CO_EINVAL, "InsertOrAssign needs a map (value_bytes > 0)");
+    return insert_impl(t, pairs, nullptr, false, n, true, s, nullptr, nullptr);
+}
+
+int b2co_oa_assign_if_async(b2co_oa_table* t, void const* pairs, uint8_t const* stencil, uint64_t n, b2co_stream s)
+{
+    if (int st = check_table(t)) return st;
+    if (t->desc.value_bytes == 0) return fail(B2CO_EINVAL, "AssignIf needs a map (value_bytes > 0)");
+    if (n == 0 || !pairs || !stencil) return B2CO_OK;
+    if (int st = check_batch(n)) return st;
+    return t->ops->assign_if(t->args, t->desc.bucket_size, pairs, stencil, uint32_t(n), cs(s));
+}
+
+int b2co_oa_insert_and_find_async(b2co_oa_table* t, void const* pairs, void* out_found, uint8_t* out_inserted,
+                                  uint64_t n, int mode, b2co_stream s)
+{
+    if (int st = check_table(t)) return st;
+    if (n == 0 || !pairs) return B2CO_OK;
+    if (!out_found || !out_inserted) return fail(B2CO_EINVAL, "InsertAndFind outputs must not be null");
+    if (int st = check_batch(n)) return st;
+    if (mode == B2CO_IAF_RACE)
+        return t->ops->iaf_race(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), cs(s));
+    if (mode != B2CO_IAF_FIRST_WINS) return fail(B2CO_EINVAL, "unknown InsertAndFind mode");
+    if (int st = ensure_first_wins_scratch(t, n)) return st;
+    B2CO_CUDA(cudaMemsetAsync(t->d_newbits, 0, ((t->capacity + 31) / 32) * 4, cs(s)));
+    return t->ops->iaf_first(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), t->d_pos,
+                             t->d_newbits, t->d_owner, cs(s));
+}
+
+int b2co_oa_insert_and_find(b2co_oa_table* t, void const* pairs, void* out_found, uint8_t* out_inserted, uint64_t n,
+                            int mode, b2co_stream s)
+{
+    if (int st = b2co_oa_insert_and_find_async(t, pairs, out_found, out_inserted, n, mode, s)) return st;
+    B2CO_CUDA(cudaStreamSynchronize(cs(s)));
+    return B2CO_OK;
+}
+
+// ---- erase / count ---------------------------------------------------------
+
+static int erase_impl(b2co_oa_table* t, void const* keys, uint64_t n, b2co_stream s, uint64_t* failed)
+{
+    if (failed) *failed = 0;
+    if (int st = check_table(t)) return st;
+    if (n == 0) return B2CO_OK;
+    if (!keys) {
+        if (failed) *failed = n;
+        return B2CO_OK;
+    }
+    if (int st = check_batch(n)) return st;
+    cudaStream_t c = cs(s);
+    if (failed) B2CO_CUDA(cudaMemsetAsync(t->d_counters, 0, sizeof(unsigned long long), c));
+    int st = t->ops->erase(t->args, t->desc.bucket_size, keys, uint32_t(n), failed ? t->d_counters : nullptr, c);
+    if (st || !failed) return st;
+    if ((st = sync_counters(t, c, 1))) return st;
+    *failed = t->h_counters[0];
+    return B2CO_OK;
+}
+
+int b2co_oa_erase(b2co_oa_table* t, void const* keys, uint64_t n, b2co_stream s, uint64_t* failed)
+{
+    uint64_t dummy;
+    return erase_impl(t, keys, n, s, failed ? failed : &dummy);
+}
+
+int b2co_oa_erase_async(b2co_oa_table* t, void const* keys, uint64_t n, b2co_stream s)
+{
+    return erase_impl(t, keys, n, s, nullptr);
+}
+
+int b2co_oa_count(b2co_oa_table* t, void const* keys, uint64_t n, b2co_stream s, uint64_t* count)
+{
+    if (!count) return fail(B2CO_EINVAL, "null output");
+    *count = 0;
+    if (int st = check_table(t)) return st;
+    if (n == 0 || !keys) return B2CO_OK;
+    if (int st = check_batch(n)) return st;
+    cudaStream_t c = cs(s);
+    B2CO_CUDA(cudaMemsetAsync(t->d_counters, 0, sizeof(unsigned long long), c));
+    int st = t->ops->count(t->args, t->desc.bucket_size, keys, uint32_t(n), t->d_counters, c);
+    if (st) return st;
+    if ((st = sync_counters(t, c, 1))) return st;
+    *count = t->h_counters[0];
+    return B2CO_OK;
+}
+
+// ---- lookups -----------------------------------------------------------------
+
+static int lookup_async(b2co_oa_table* t, bool contains, void const* keys, uint8_t const* stencil, bool use_stencil,
+                        void* out, uint64_t n, b2co_stream s)
+{
+    if (int st = check_table(t)) return st;
+    if (n == 0 || !keys || !out || (use_stencil && !stencil)) return B2CO_OK;
+    if (int st = check_batch(n)) return st;
+    return launch_find(t, contains, keys, stencil, out, n, cs(s));
+}
+
+static int lookup_sync(b2co_oa_table* t, bool contains, void const* keys, uint8_t const* stencil, bool use_stencil,
+                       void* out, uint64_t n, b2co_stream s)
+{
+    if (int st = lookup_async(t, contains, keys, stencil, use_stencil, out, n, s)) return st;
+    B2CO_CUDA(cudaStreamSynchronize(cs(s)));
+    return B2CO_OK;
+}
+
+int b2co_oa_find(b2co_oa_table* t, void const* k, void* o, uint64_t n, b2co_stream s)
+{
+    return lookup_sync(t, false, k, nullptr, false, o, n, s);
+}
+int b2co_oa_find_async(b2co_oa_table* t, void const* k, void* o, uint64_t n, b2co_stream s)
+{
+    return lookup_async(t, false, k, nullptr, false, o, n, s);
+}
+int b2co_oa_find_if(b2co_oa_table* t, void const* k, uint8_t const* st, void* o, uint64_t n, b2co_stream s)
+{
+    return lookup_sync(t, false, k, st, true, o, n, s);
+}
+int b2co_oa_find_if_async(b2co_oa_table* t, void const* k, uint8_t const* st, void* o, uint64_t n, b2co_stream s)
+{
+    return lookup_async(t, false, k, st, true, o, n, s);
+}
+int b2co_oa_contains(b2co_oa_table* t, void const* k, uint8_t* o, uint64_t n, b2co_stream s)
+{
+    return lookup_sync(t, true, k, nullptr, false, o, n, s);
+}
+int b2co_oa_contains_async(b2co_oa_table* t, void const* k, uint8_t* o, uint64_t n, b2co_stream s)
+{
+    return lookup_async(t, true, k, nullptr, false, o, n, s);
+}
+int b2co_oa_contains_if(b2co_oa_table* t, void const* k, uint8_t const* st, uint8_t* o, uint64_t n, b2co_stream s)
+{
+    return lookup_sync(t, true, k, st, true, o, n, s);
+}
+int b2co_oa_contains_if_async(b2co_oa_table* t, void const* k, uint8_t const* st, uint8_t* o, uint64_t n,
+                              b2co_stream s)
+{
+    return lookup_async(t, true, k, st, true, o, n, s);
+}
+
+int b2co_oa_set_find_shape(b2co_oa_table* t, uint32_t lanes, uint32_t items)
+{
+    if (int st = check_table(t)) return st;
+    if (lanes == 0 && items == 0) {
+        default_shape(t);
+        return B2CO_OK;
+    }
+    if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) return fail(B2CO_EINVAL, "lanes must be 1, 2, 4 or 8");
+    if (items != 1 && items != 2 && items != 4) return fail(B2CO_EINVAL, "keys per lane must be 1, 2 or 4");
+    t->find_lanes = lanes;
+    t->find_items = items;
+    return B2CO_OK;
+}
+
+// Host-buffer Find: chunks alternate between two pipeline streams, each chunk
+// copy-in -> probe -> copy-out in stream order, so chunk c+1's copy-in overlaps
+// chunk c's probe and copy-out.  Pinned host buffers give full overlap.
+int b2co_oa_find_host(b2co_oa_table* t, void const* host_keys, void* host_out, uint64_t n, b2co_stream s)
+{
+    if (int st = check_table(t)) return st;
+    if (n == 0 || !host_keys || !host_out) return B2CO_OK;
+    uint32_t const kb = t->desc.key_bytes;
+    uint32_t const ob = t->desc.value_bytes ? t->desc.value_bytes : kb;
+    uint64_t const chunk = 1ull << 24;  // keys per chunk
+    if (!t->stage) {
+        t->stage_keys = chunk;
+        B2CO_CUDA(cudaMalloc(&t->stage, 2 * chunk * (kb + ob)));
+        for (auto& p : t->pipe) B2CO_CUDA(cudaStreamCreateWithFlags(&p, cudaStreamNonBlocking));
+        for (auto& e : t->ev) B2CO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t c = cs(s);
+    B2CO_CUDA(cudaEventRecord(t->ev[2], c));
+    for (auto& p : t->pipe) B2CO_CUDA(cudaStreamWaitEvent(p, t->ev[2], 0));
+    char* base = static_cast<char*>(t->stage);
+    for (uint64_t off = 0, c_i = 0; off < n; off += chunk, ++c_i) {
+        uint64_t m = n - off < chunk ? n - off : chunk;
+        int slot = int(c_i & 1);
+        cudaStream_t p = t->pipe[slot];
+        char* dk = base + uint64_t(slot) * chunk * (kb + ob);
+        char* dout = dk + chunk * kb;
+        B2CO_CUDA(cudaMemcpyAsync(dk, static_cast<char const*>(host_keys) + off * kb, m * kb,
+                                  cudaMemcpyHostToDevice, p));
+        if (int st = launch_find(t, false, dk, nullptr, dout, m, p)) return st;
+        B2CO_CUDA(cudaMemcpyAsync(static_cast<char*>(host_out) + off * ob, dout, m * ob, cudaMemcpyDeviceToHost, p));
+    }
+    for (int i = 0; i < 2; ++i) {
+        B2CO_CUDA(cudaEventRecord(t->ev[i], t->pipe[i]));
+        B2CO_CUDA(cudaStreamWaitEvent(c, t->ev[i], 0));
+    }
+    B2CO_CUDA(cudaStreamSynchronize(c));
+    return B2CO_OK;
+}
+
+}  // extern "C"

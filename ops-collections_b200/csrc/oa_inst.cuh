@@ -1,0 +1,152 @@
+// oa_inst.cuh -- launchers of the open-addressing kernels for one slot layout.
+// Each oa_slot_*.cu instantiates this for one layout so the six layouts
+// compile in parallel.
+#pragma once
+
+#include "b2co_host.h"
+#include "oa_kernels.cuh"
+
+namespace b2co {
+
+template <class S>
+struct OaImpl {
+    static constexpr uint32_t kBlock = 256;
+
+    template <class F>
+    static int with_b(uint32_t b, F&& f)
+    {
+        switch (b) {
+            case 1: return f(std::integral_constant<int, 1>{});
+            case 2: return f(std::integral_constant<int, 2>{});
+            case 4: return f(std::integral_constant<int, 4>{});
+            case 5: return f(std::integral_constant<int, 5>{});
+            case 8: return f(std::integral_constant<int, 8>{});
+        }
+        return fail(B2CO_EINVAL, "unsupported bucket size");
+    }
+
+    static int check_launch(char const* what)
+    {
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? B2CO_OK : cuda_fail(e, what);
+    }
+
+    static int clear(OaArgs const& a, cudaStream_t s)
+    {
+        auto k = k_clear<S>;
+        k<<<grid_for((void const*)k, kBlock, a.probe.capacity, kBlock * 4), kBlock, 0, s>>>(
+            a.slots, a.probe.capacity, a.empty_key, a.empty_value);
+        return check_launch("clear kernel");
+    }
+
+    static int insert(OaArgs const& a, uint32_t b, void const* pairs, uint8_t const* stencil, uint32_t n,
+                      bool assign, unsigned long long* counters, cudaStream_t s)
+    {
+        return with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            auto k = assign ? k_insert<S, B, true> : k_insert<S, B, false>;
+            k<<<grid_for((void const*)k, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, stencil, n, counters);
+            return check_launch("insert kernel");
+        });
+    }
+
+    static int assign_if(OaArgs const& a, uint32_t b, void const* pairs, uint8_t const* stencil, uint32_t n,
+                         cudaStream_t s)
+    {
+        return with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            auto k = k_assign_if<S, B>;
+            k<<<grid_for((void const*)k, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, stencil, n);
+            return check_launch("assign kernel");
+        });
+    }
+
+    static int iaf_race(OaArgs const& a, uint32_t b, void const* pairs, void* found, uint8_t* inserted, uint32_t n,
+                        cudaStream_t s)
+    {
+        return with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            auto k = k_iaf_race<S, B>;
+            k<<<grid_for((void const*)k, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, found, inserted, n);
+            return check_launch("insert_and_find kernel");
+        });
+    }
+
+    static int iaf_first(OaArgs const& a, uint32_t b, void const* pairs, void* found, uint8_t* inserted,
+                         uint32_t n, uint32_t* pos, uint32_t* newbits, uint32_t* owner, cudaStream_t s)
+    {
+        return with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            auto k1 = k_iaf_place<S, B>;
+            k1<<<grid_for((void const*)k1, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, n, pos, newbits, owner);
+            auto k2 = k_iaf_min<S>;
+            k2<<<grid_for((void const*)k2, kBlock, n, kBlock), kBlock, 0, s>>>(pos, newbits, owner, n);
+            auto k3 = k_iaf_final<S>;
+            k3<<<grid_for((void const*)k3, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, pos, newbits, owner, found,
+                                                                                inserted, n);
+            return check_launch("insert_and_find (first wins) kernels");
+        });
+    }
+
+    template <int B, bool C>
+    static int find_shape(OaArgs const& a, uint32_t lanes, uint32_t items, void const* keys, uint8_t const* stencil,
+                          void* out, uint32_t n, cudaStream_t s)
+    {
+        void (*k)(OaArgs, void const*, uint8_t const*, void*, uint32_t) = nullptr;
+        uint64_t per_block = kBlock;
+        if (B == 1 || lanes <= 1) {
+            if (items >= 4) k = k_find_lane<S, B, 4, C>, per_block *= 4;
+            else if (items == 2) k = k_find_lane<S, B, 2, C>, per_block *= 2;
+            else k = k_find_lane<S, B, 1, C>;
+        } else if (lanes == 2) {
+            k = k_find_tile<S, B, 2, C>, per_block /= 2;
+        } else if (lanes == 4) {
+            k = k_find_tile<S, B, 4, C>, per_block /= 4;
+        } else {
+            k = k_find_tile<S, B, 8, C>, per_block /= 8;
+        }
+        k<<<grid_for((void const*)k, kBlock, n, per_block), kBlock, 0, s>>>(a, keys, stencil, out, n);
+        return check_launch(C ? "contains kernel" : "find kernel");
+    }
+
+    static int find(OaArgs const& a, uint32_t b, uint32_t lanes, uint32_t items, bool contains, void const* keys,
+                    uint8_t const* stencil, void* out, uint32_t n, cudaStream_t s)
+    {
+        return with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            return contains ? find_shape<B, true>(a, lanes, items, keys, stencil, out, n, s)
+                            : find_shape<B, false>(a, lanes, items, keys, stencil, out, n, s);
+        });
+    }
+
+    static int erase(OaArgs const& a, uint32_t b, void const* keys, uint32_t n, unsigned long long* counters,
+                     cudaStream_t s)
+    {
+        return with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            auto k = k_erase<S, B>;
+            k<<<grid_for((void const*)k, kBlock, n, kBlock), kBlock, 0, s>>>(a, keys, n, counters);
+            return check_launch("erase kernel");
+        });
+    }
+
+    static int count(OaArgs const& a, uint32_t b, void const* keys, uint32_t n, unsigned long long* counter,
+                     cudaStream_t s)
+    {
+        return with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            auto k = k_count<S, B>;
+            k<<<grid_for((void const*)k, kBlock, n, kBlock), kBlock, 0, s>>>(a, keys, n, counter);
+            return check_launch("count kernel");
+        });
+    }
+
+    static constexpr OaOps ops{&clear, &insert, &assign_if, &iaf_race, &iaf_first, &find, &erase, &count};
+};
+
+}  // namespace b2co
+
+#define B2CO_DEFINE_OA_OPS(NAME, KB, VB) \
+    namespace b2co {                     \
+    OaOps const NAME = OaImpl<SlotT<KB, VB>>::ops; \
+    }

@@ -1,0 +1,632 @@
+// oa_kernels.cuh -- sm_100a kernels for the open-addressing containers
+// (StaticMap / StaticSet / DynamicMap submaps).
+//
+// Per-key algorithms restate detail/open_addressing/open_addressing_ref_impl.h:
+// probe bucket windows from the scheme's start index; inside a window scan the
+// slots in order; an empty-key slot ends a lookup (or is claimed by an insert),
+// an equal key is a hit/duplicate; a full cycle of the probe sequence fails.
+//
+// B200 design:
+//  * a slot is published with ONE atomic CAS of the whole slot (32/64/128-bit),
+//    so the key and payload appear together and no reader ever waits for a
+//    payload (the reference's unbounded WaitForPayload spin does not exist);
+//  * lookups read the table through the non-coherent path with 16-byte vector
+//    loads, either one lane per key (all B slots of the window issued back to
+//    back, several keys per lane in flight) or G lanes per key (one slot per
+//    lane, the window resolved with warp ballots);
+//  * every loop is bounded by the probe cycle, so no kernel can spin.
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+
+#include "b2co_common.cuh"
+
+namespace b2co {
+
+constexpr uint32_t kNoSlot = 0xffffffffu;
+
+struct OaArgs {
+    void* slots;
+    ProbeParams probe;
+    uint64_t empty_key;
+    uint64_t empty_value;
+    uint64_t erased_key;
+};
+
+template <int N>
+using WordT = typename std::conditional<N == 8, unsigned long long, uint32_t>::type;
+
+template <class S>
+struct Io {
+    static constexpr int PB = S::is_set ? S::key_bytes : S::value_bytes;  // payload bytes
+    using Key = WordT<S::key_bytes>;
+    using Payload = WordT<PB>;
+    using Raw = typename S::Raw;
+    __device__ static uint64_t load_key(void const* keys, uint32_t i)
+    {
+        return uint64_t(__ldg(reinterpret_cast<Key const*>(keys) + i));
+    }
+    __device__ static void store_payload(void* out, uint32_t i, uint64_t v)
+    {
+        reinterpret_cast<Payload*>(out)[i] = Payload(v);
+    }
+    __device__ static Raw load_pair(void const* pairs, uint32_t i) { return ld_ro(reinterpret_cast<Raw const*>(pairs) + i); }
+};
+
+template <class S>
+__device__ __forceinline__ uint64_t empty_payload(OaArgs const& a)
+{
+    return S::is_set ? a.empty_key : a.empty_value;
+}
+
+// The slot to CAS an insert against.  Slots up to 8 bytes compare the whole
+// canonical empty pair (PackCas, open_addressing_ref_impl.h:126-147); 16-byte
+// slots compare the key only (CasDependentWrite, :164-185), which here means
+// "the slot exactly as loaded, whose key was seen empty".
+template <class S>
+__device__ __forceinline__ bool insert_expected(OaArgs const& a, typename S::Raw cur, typename S::Raw& expected)
+{
+    if constexpr (S::bytes == 16) {
+        expected = cur;
+        return true;
+    } else {
+        expected = S::make(a.empty_key, a.empty_value);
+        return raw_eq(cur, expected);
+    }
+}
+
+// The slot written by an insert: key and payload, the rest of the slot kept.
+template <class S>
+__device__ __forceinline__ typename S::Raw insert_desired(typename S::Raw cur, uint64_t k, uint64_t v)
+{
+    if constexpr (S::bytes == 16) {
+        U128 r = cur;
+        r.lo = (r.lo & ~S::kmask) | (k & S::kmask);
+        if constexpr (S::value_offset == 8) r.hi = (r.hi & ~S::vmask) | (v & S::vmask);
+        return r;
+    } else {
+        return S::make(k, v);
+    }
+}
+
+// Payload store of an existing key (AssignPayload, open_addressing_ref_impl.h:208-220):
+// a whole-slot store for slots up to 8 bytes, the payload field otherwise.
+template <class S>
+__device__ __forceinline__ void assign_payload(typename S::Raw* slot, uint64_t k, uint64_t v)
+{
+    if constexpr (S::is_set) {
+        return;
+    } else if constexpr (S::bytes == 8) {
+        *reinterpret_cast<volatile unsigned long long*>(slot) = (unsigned long long)S::make(k, v);
+    } else if constexpr (S::value_bytes == 8) {
+        reinterpret_cast<volatile unsigned long long*>(slot)[1] = v;
+    } else {
+        reinterpret_cast<volatile uint32_t*>(slot)[2] = uint32_t(v);
+    }
+}
+
+// A 16-byte slot seen through a plain vector load could in principle be torn
+// against a concurrent 128-bit CAS.  Only a key-matching slot whose payload
+// still reads as the empty payload is ambiguous; re-read it atomically.
+template <class S>
+__device__ __forceinline__ typename S::Raw settle(OaArgs const& a, typename S::Raw* slot, typename S::Raw cur)
+{
+    if constexpr (S::bytes == 16 && !S::is_set) {
+        if (S::value(cur) == (a.empty_value & S::vmask)) return cas_slot(slot, cur, cur);
+    }
+    return cur;
+}
+
+// ----------------------------------------------------------------------------
+// Insert / InsertIf / InsertOrAssign
+// (InsertVerdict, open_addressing_ref_impl.h:489-532; kernels.h:46-182)
+// ----------------------------------------------------------------------------
+
+enum { kFailed = 0, kSuccess = 1, kDuplicate = 2 };
+
+template <class S, int B, bool ASSIGN>
+__device__ __forceinline__ int insert_one(OaArgs const& a, uint64_t key, uint64_t val)
+{
+    using Raw = typename S::Raw;
+    if (key == a.empty_key) return kFailed;
+    Raw* slots = reinterpret_cast<Raw*>(a.slots);
+    uint32_t const init = probe_init<S::key_bytes, B>(a.probe, key);
+    uint32_t idx = init, step = 0;
+    for (;;) {
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            Raw* sp = slots + idx + j;
+            Raw cur = ld_rw(sp);
+            uint64_t k = S::key(cur);
+            if (k == key) {
+                if constexpr (ASSIGN) assign_payload<S>(sp, key, val);
+                return kDuplicate;
+            }
+            if (k == a.empty_key) {
+                Raw expected;
+                if (!insert_expected<S>(a, cur, expected)) continue;
+                Raw old = cas_slot(sp, expected, insert_desired<S>(cur, key, val));
+                if (raw_eq(old, expected)) return kSuccess;
+                if (S::key(old) == key) {
+                    if constexpr (ASSIGN) assign_payload<S>(sp, key, val);
+                    return kDuplicate;
+                }
+            }
+        }
+        if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
+        idx = probe_next(idx, step, a.probe.capacity);
+        if (idx == init) return kFailed;
+    }
+}
+
+__device__ __forceinline__ void warp_add_counter(unsigned long long* counter, uint32_t v)
+{
+    uint32_t sum = __reduce_add_sync(0xffffffffu, v);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(counter, (unsigned long long)sum);
+}
+
+// counters[0] += failed, counters[1] += assigned (NULL counters = async form).
+template <class S, int B, bool ASSIGN>
+__global__ void __launch_bounds__(256) k_insert(OaArgs a, void const* pairs, uint8_t const* stencil, uint32_t n,
+                                                unsigned long long* counters)
+{
+    uint32_t failed = 0, assigned = 0;
+    uint32_t const stride = gridDim.x * blockDim.x;
+    // warp-uniform trip count so the counter reduction sees every lane
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        uint32_t i = base + (threadIdx.x & 31);
+        if (i < n && (!stencil || stencil[i])) {
+            typename S::Raw p = Io<S>::load_pair(pairs, i);
+            int r = insert_one<S, B, ASSIGN>(a, S::key(p), S::value(p));
+            failed += r == kFailed;
+            assigned += r == kDuplicate;
+        }
+    }
+    if (counters) {
+        warp_add_counter(counters, failed);
+        if (ASSIGN) warp_add_counter(counters + 1, assigned);
+    }
+}
+
+// AssignIf (Assign, open_addressing_ref_impl.h:384-410): payload overwrite of
+// existing keys only; an empty slot ends the search.
+template <class S, int B>
+__global__ void __launch_bounds__(256) k_assign_if(OaArgs a, void const* pairs, uint8_t const* stencil, uint32_t n)
+{
+    using Raw = typename S::Raw;
+    Raw* slots = reinterpret_cast<Raw*>(a.slots);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (stencil && !stencil[i]) continue;
+        Raw p = Io<S>::load_pair(pairs, i);
+        uint64_t key = S::key(p);
+        uint32_t const init = probe_init<S::key_bytes, B>(a.probe, key);
+        uint32_t idx = init, step = 0;
+        bool done = false;
+        while (!done) {
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                if (done) break;
+                Raw* sp = slots + idx + j;
+                uint64_t k = S::key(ld_rw(sp));
+                if (k == a.empty_key) done = true;
+                else if (k == key) {
+                    assign_payload<S>(sp, key, S::value(p));
+                    done = true;
+                }
+            }
+            if (done) break;
+            if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
+            idx = probe_next(idx, step, a.probe.capacity);
+            if (idx == init) break;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// InsertAndFind, race mode: exactly the reference's concurrent semantics
+// (open_addressing_ref_impl.h:301-330, 543-565); duplicates in one batch race.
+// ----------------------------------------------------------------------------
+
+template <class S, int B>
+__global__ void __launch_bounds__(256) k_iaf_race(OaArgs a, void const* pairs, void* out_found,
+                                                  uint8_t* out_inserted, uint32_t n)
+{
+    using Raw = typename S::Raw;
+    Raw* slots = reinterpret_cast<Raw*>(a.slots);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Raw p = Io<S>::load_pair(pairs, i);
+        uint64_t key = S::key(p), val = S::value(p);
+        uint64_t found = empty_payload<S>(a);
+        uint8_t inserted = 0;
+        if (key != a.empty_key) {
+            uint32_t const init = probe_init<S::key_bytes, B>(a.probe, key);
+            uint32_t idx = init, step = 0;
+            bool done = false;
+            while (!done) {
+#pragma unroll
+                for (int j = 0; j < B; ++j) {
+                    if (done) break;
+                    Raw* sp = slots + idx + j;
+                    Raw cur = ld_rw(sp);
+                    uint64_t k = S::key(cur);
+                    if (k == key) {
+                        found = S::value(settle<S>(a, sp, cur));
+                        done = true;
+                    } else if (k == a.empty_key) {
+                        Raw expected;
+                        if (!insert_expected<S>(a, cur, expected)) continue;
+                        Raw old = cas_slot(sp, expected, insert_desired<S>(cur, key, val));
+                        if (raw_eq(old, expected)) {
+                            found = S::is_set ? key : val;
+                            inserted = 1;
+                            done = true;
+                        } else if (S::key(old) == key) {
+                            found = S::value(old);
+                            done = true;
+                        }
+                    }
+                }
+                if (done) break;
+                if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
+                idx = probe_next(idx, step, a.probe.capacity);
+                if (idx == init) break;
+            }
+        }
+        Io<S>::store_payload(out_found, i, found);
+        out_inserted[i] = inserted;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// InsertAndFind, first-wins mode: deterministic, equal to inserting the batch
+// sequentially in input order (the golden of tests/common/golden.h:104-131).
+//   place : every key finds or claims its slot; pos[i] = slot; a claiming
+//           thread marks the slot new and records itself as its owner;
+//   min   : inputs that landed on a new slot lower the owner to the least
+//           input index (atomicMin);
+//   final : owner i is the inserted one; every other input on a new slot
+//           finds the owner's payload (read from the input, never a racing
+//           slot); inputs on old slots find the stored payload.
+// ----------------------------------------------------------------------------
+
+template <class S, int B>
+__global__ void __launch_bounds__(256) k_iaf_place(OaArgs a, void const* pairs, uint32_t n, uint32_t* pos,
+                                                   uint32_t* newbits, uint32_t* owner)
+{
+    using Raw = typename S::Raw;
+    Raw* slots = reinterpret_cast<Raw*>(a.slots);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Raw p = Io<S>::load_pair(pairs, i);
+        uint64_t key = S::key(p), val = S::value(p);
+        uint32_t where = kNoSlot;
+        if (key != a.empty_key) {
+            uint32_t const init = probe_init<S::key_bytes, B>(a.probe, key);
+            uint32_t idx = init, step = 0;
+            bool done = false;
+            while (!done) {
+#pragma unroll
+                for (int j = 0; j < B; ++j) {
+                    if (done) break;
+                    Raw* sp = slots + idx + j;
+                    Raw cur = ld_rw(sp);
+                    uint64_t k = S::key(cur);
+                    if (k == key) {
+                        where = idx + j;
+                        done = true;
+                    } else if (k == a.empty_key) {
+                        Raw expected;
+                        if (!insert_expected<S>(a, cur, expected)) continue;
+                        Raw old = cas_slot(sp, expected, insert_desired<S>(cur, key, val));
+                        if (raw_eq(old, expected)) {
+                            where = idx + j;
+                            atomicOr(newbits + (where >> 5), 1u << (where & 31));
+                            owner[where] = i;
+                            done = true;
+                        } else if (S::key(old) == key) {
+                            where = idx + j;
+                            done = true;
+                        }
+                    }
+                }
+                if (done) break;
+                if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
+                idx = probe_next(idx, step, a.probe.capacity);
+                if (idx == init) break;
+            }
+        }
+        pos[i] = where;
+    }
+}
+
+__device__ __forceinline__ bool bit_set(uint32_t const* bits, uint32_t s) { return (bits[s >> 5] >> (s & 31)) & 1u; }
+
+template <class S>  // one copy per slot layout's translation unit
+__global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t const* newbits, uint32_t* owner,
+                                                 uint32_t n)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t s = pos[i];
+        if (s != kNoSlot && bit_set(newbits, s) && owner[s] != i) atomicMin(owner + s, i);
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_iaf_final(OaArgs a, void const* pairs, uint32_t const* pos,
+                                                   uint32_t const* newbits, uint32_t const* owner, void* out_found,
+                                                   uint8_t* out_inserted, uint32_t n)
+{
+    using Raw = typename S::Raw;
+    Raw* slots = reinterpret_cast<Raw*>(a.slots);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t s = pos[i];
+        uint64_t found = empty_payload<S>(a);
+        uint8_t inserted = 0;
+        if (s != kNoSlot) {
+            if (bit_set(newbits, s)) {
+                uint32_t m = owner[s];
+                Raw pm = Io<S>::load_pair(pairs, m);
+                found = S::value(pm);
+                if (m == i) {
+                    inserted = 1;
+                    assign_payload<S>(slots + s, S::key(pm), found);
+                }
+            } else {
+                found = S::value(ld_rw(slots + s));
+            }
+        }
+        Io<S>::store_payload(out_found, i, found);
+        out_inserted[i] = inserted;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Find / Contains (FindAndContains, open_addressing_ref_impl.h:567-605)
+// ----------------------------------------------------------------------------
+
+// First slot of a loaded window that ends the scan (empty or equal), -1 if none.
+template <class S, int B>
+__device__ __forceinline__ int scan_window(typename S::Raw const (&w)[B], uint64_t key, uint64_t empty_key)
+{
+    int stop = -1;
+#pragma unroll
+    for (int j = B - 1; j >= 0; --j) {
+        uint64_t k = S::key(w[j]);
+        if (k == empty_key || k == key) stop = j;
+    }
+    return stop;
+}
+
+template <class S, int B>
+__device__ __forceinline__ void load_window(typename S::Raw const* slots, uint32_t idx, typename S::Raw (&w)[B])
+{
+#pragma unroll
+    for (int j = 0; j < B; ++j) w[j] = ld_ro(slots + idx + j);
+}
+
+// Continue a lookup whose first window held neither the key nor an empty slot.
+template <class S, int B>
+__device__ __noinline__ bool find_rest(OaArgs const& a, uint64_t key, uint32_t init, uint64_t& payload)
+{
+    using Raw = typename S::Raw;
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t const step = probe_step<S::key_bytes, B>(a.probe, key);
+    uint32_t idx = probe_next(init, step, a.probe.capacity);
+    while (idx != init) {
+        Raw w[B];
+        load_window<S, B>(slots, idx, w);
+        int j = scan_window<S, B>(w, key, a.empty_key);
+        if (j >= 0) {
+            bool hit = S::key(w[j]) == key;
+            payload = hit ? S::value(w[j]) : empty_payload<S>(a);
+            return hit;
+        }
+        idx = probe_next(idx, step, a.probe.capacity);
+    }
+    payload = empty_payload<S>(a);
+    return false;
+}
+
+// One lane per key, ITEMS keys per lane in flight: all windows are loaded
+// before any is resolved, so a lane keeps ITEMS * B independent loads open.
+template <class S, int B, int ITEMS, bool CONTAINS>
+__global__ void __launch_bounds__(256) k_find_lane(OaArgs a, void const* keys, uint8_t const* stencil, void* out,
+                                                   uint32_t n)
+{
+    using Raw = typename S::Raw;
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t const stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + threadIdx.x; base < n; base += stride * ITEMS) {
+        uint64_t key[ITEMS];
+        uint32_t init[ITEMS];
+        bool live[ITEMS];
+        Raw w[ITEMS][B];
+#pragma unroll
+        for (int t = 0; t < ITEMS; ++t) {
+            uint32_t i = base + t * stride;
+            live[t] = i < n && (!stencil || stencil[i]);
+            key[t] = live[t] ? Io<S>::load_key(keys, i) : 0;
+            init[t] = live[t] ? probe_init<S::key_bytes, B>(a.probe, key[t]) : 0;
+        }
+#pragma unroll
+        for (int t = 0; t < ITEMS; ++t)
+            if (live[t]) load_window<S, B>(slots, init[t], w[t]);
+#pragma unroll
+        for (int t = 0; t < ITEMS; ++t) {
+            uint32_t i = base + t * stride;
+            if (i >= n) continue;
+            uint64_t payload = empty_payload<S>(a);
+            bool hit = false;
+            if (live[t]) {
+                int j = scan_window<S, B>(w[t], key[t], a.empty_key);
+                if (j >= 0) {
+                    hit = S::key(w[t][j]) == key[t];
+                    if (hit) payload = S::value(w[t][j]);
+                } else {
+                    hit = find_rest<S, B>(a, key[t], init[t], payload);
+                }
+            }
+            if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = hit;
+            else Io<S>::store_payload(out, i, payload);
+        }
+    }
+}
+
+// G lanes per key: lane r of a tile loads slots r, r+G, ... of the window; the
+// tile resolves the window with one ballot pair per round and the lane holding
+// the hit slot hands its payload to the tile's first lane, which writes it.
+template <class S, int B, int G, bool CONTAINS>
+__global__ void __launch_bounds__(256) k_find_tile(OaArgs a, void const* keys, uint8_t const* stencil, void* out,
+                                                   uint32_t n)
+{
+    using Raw = typename S::Raw;
+    constexpr int ROUNDS = (B + G - 1) / G;
+    constexpr uint32_t TILES = 32 / G;
+    constexpr uint32_t TILE_MASK = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t const lane = threadIdx.x & 31, r = lane % G, tile_shift = (lane / G) * G;
+    uint32_t const warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * TILES; base < n; base += warps * TILES) {
+        uint32_t const i = base + lane / G;
+        bool const live = i < n && (!stencil || stencil[i]);
+        uint64_t const key = live ? Io<S>::load_key(keys, i) : 0;
+        uint32_t const init = live ? probe_init<S::key_bytes, B>(a.probe, key) : 0;
+        uint32_t idx = init, step = 0;
+        bool done = !live, hit = false;
+        int stop_j = -1;
+        uint64_t payload = empty_payload<S>(a);
+        while (__any_sync(0xffffffffu, !done)) {
+            uint32_t stop_bits = 0, hit_bits = 0;
+            Raw w[ROUNDS];
+#pragma unroll
+            for (int t = 0; t < ROUNDS; ++t) {
+                int j = int(r) + t * G;
+                bool own = !done && j < B;
+                uint64_t k = 0;
+                if (own) {
+                    w[t] = ld_ro(slots + idx + j);
+                    k = S::key(w[t]);
+                }
+                bool is_hit = own && k == key;
+                bool is_stop = own && (k == a.empty_key || is_hit);
+                stop_bits |= ((__ballot_sync(0xffffffffu, is_stop) >> tile_shift) & TILE_MASK) << (t * G);
+                hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> tile_shift) & TILE_MASK) << (t * G);
+            }
+            if (!done) {
+                if (stop_bits) {
+                    stop_j = __ffs(stop_bits) - 1;
+                    hit = (hit_bits >> stop_j) & 1u;
+                    done = true;
+                    if (hit && int(r) == stop_j % G) {
+#pragma unroll
+                        for (int t = 0; t < ROUNDS; ++t)
+                            if (t == stop_j / G) payload = S::value(w[t]);
+                    }
+                } else {
+                    if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
+                    idx = probe_next(idx, step, a.probe.capacity);
+                    if (idx == init) done = true;
+                }
+            }
+        }
+        uint32_t const src = tile_shift + (stop_j >= 0 ? uint32_t(stop_j % G) : 0u);
+        uint64_t const pv = __shfl_sync(0xffffffffu, (unsigned long long)payload, src);
+        if (r == 0 && i < n) {
+            if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = hit;
+            else Io<S>::store_payload(out, i, hit ? pv : empty_payload<S>(a));
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Erase (open_addressing_ref_impl.h:340-379) and Count (kernels.h:427-467)
+// ----------------------------------------------------------------------------
+
+template <class S, int B>
+__global__ void __launch_bounds__(256) k_erase(OaArgs a, void const* keys, uint32_t n, unsigned long long* counters)
+{
+    using Raw = typename S::Raw;
+    Raw* slots = reinterpret_cast<Raw*>(a.slots);
+    bool const tomb = a.erased_key != a.empty_key;
+    uint64_t const target_key = tomb ? a.erased_key : a.empty_key;
+    uint32_t failed = 0;
+    uint32_t const stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        uint32_t i = base + (threadIdx.x & 31);
+        if (i >= n) continue;
+        uint64_t key = Io<S>::load_key(keys, i);
+        uint32_t const init = probe_init<S::key_bytes, B>(a.probe, key);
+        uint32_t idx = init, step = 0;
+        bool done = false, ok = false;
+        while (!done) {
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                if (done) break;
+                Raw* sp = slots + idx + j;
+                Raw cur = ld_rw(sp);
+                uint64_t k = S::key(cur);
+                if (k == a.empty_key) {
+                    // only a configured tombstone lets an empty slot end the search
+                    if (tomb) done = true;
+                    continue;
+                }
+                if (k == key) {
+                    Raw desired;
+                    if constexpr (S::bytes == 16) desired = insert_desired<S>(cur, target_key, a.empty_value);
+                    else desired = S::make(target_key, a.empty_value);
+                    Raw old = cas_slot(sp, cur, desired);
+                    if (raw_eq(old, cur)) {
+                        ok = true;
+                        done = true;
+                    } else if (S::key(old) == target_key) {
+                        done = true;  // another thread erased it first
+                    }
+                }
+            }
+            if (done) break;
+            if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
+            idx = probe_next(idx, step, a.probe.capacity);
+            if (idx == init) break;
+        }
+        failed += !ok;
+    }
+    if (counters) warp_add_counter(counters, failed);
+}
+
+template <class S, int B>
+__global__ void __launch_bounds__(256) k_count(OaArgs a, void const* keys, uint32_t n, unsigned long long* counter)
+{
+    using Raw = typename S::Raw;
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t c = 0;
+    uint32_t const stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        uint32_t i = base + (threadIdx.x & 31);
+        if (i >= n) continue;
+        uint64_t key = Io<S>::load_key(keys, i);
+        uint32_t init = probe_init<S::key_bytes, B>(a.probe, key);
+        Raw w[B];
+        load_window<S, B>(slots, init, w);
+        int j = scan_window<S, B>(w, key, a.empty_key);
+        uint64_t payload;
+        if (j >= 0) c += S::key(w[j]) == key;
+        else c += find_rest<S, B>(a, key, init, payload);
+    }
+    warp_add_counter(counter, c);
+}
+
+// ----------------------------------------------------------------------------
+// Clear: every slot becomes the empty pair, padding bytes zero
+// (bucket_storage.inl:52-64, open_addressing_impl.h:478-499)
+// ----------------------------------------------------------------------------
+
+template <class S>
+__global__ void __launch_bounds__(256) k_clear(void* slots, uint32_t capacity, uint64_t empty_key, uint64_t empty_value)
+{
+    using Raw = typename S::Raw;
+    Raw const e = S::make(empty_key, empty_value);
+    Raw* s = reinterpret_cast<Raw*>(slots);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < capacity; i += gridDim.x * blockDim.x) s[i] = e;
+}
+
+}  // namespace b2co
