@@ -295,6 +295,21 @@ def run_gpu(args):
 
     q = make_queries(keys, N_QUERIES, 0.5, "torch")
     out = torch.empty(N_QUERIES, dtype=torch.int64, device="cuda")
+    if args.sweep:
+        sweep = {}
+        for lanes, items in [(1, 2), (1, 4), (2, 2), (4, 1), (4, 2), (4, 4), (8, 1), (8, 2), (8, 4)]:
+            t.set_find_shape(lanes, items)
+            for _ in range(3):
+                t.FindAsync(q, out)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(10):
+                t.FindAsync(q, out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sweep[f"{lanes}x{items}"] = round(N_QUERIES * 10 / e0.elapsed_time(e1) / 1e6, 3)
+            log(f"[sweep] lanes {lanes} items {items}: {sweep[f'{lanes}x{items}']} Gkeys/s")
+        t.set_find_shape(0, 0)
     if args.shape:
         lanes, items = (int(x) for x in args.shape.split("x"))
         t.set_find_shape(lanes, items)
@@ -319,8 +334,10 @@ def run_gpu(args):
     # exact probe-window count of the timed queries and parity on a sample, by
     # the CPU oracle over a host copy of the very same table
     extra = {}
+    if args.sweep:
+        extra["find_shape_sweep_gkeys"] = sweep
     windows_mean, cpu = None, None
-    if rank == 0:
+    if rank == 0 and not args.no_host:
         windows_mean, cpu, parity = host_side_checks(t, q, out, args)
         extra["oracle_parity_sample"] = parity
     bytes_per_query = 8 + 8 + 80 * (windows_mean if windows_mean else 1.0)
@@ -332,23 +349,7 @@ def run_gpu(args):
                 "windows_per_query": windows_mean,
                 "one_window_bound_gbs": round(N_QUERIES * 96 / (ms_per_step / 1e3) / 1e9, 1)}
 
-    # end to end through the C ABI with pinned host buffers
-    hq = q.cpu().pin_memory()
-    ho = torch.empty(N_QUERIES, dtype=torch.int64).pin_memory()
-    t.FindHost(hq.numpy(), ho.numpy())
-    torch.cuda.synchronize()
-    e2e_steps = max(3, min(args.steps, 10))
-    t0 = time.perf_counter()
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        t.FindHost(hq.numpy(), ho.numpy())
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e2e_steps
-    assert torch.equal(ho, out.cpu()), "host-buffer Find differs from device Find"
-    e2e = {"value": round(world * N_QUERIES / (e2e_ms / 1e3) / 1e9, 4), "unit": UNIT,
-           "h2d_bytes_per_step": N_QUERIES * 8, "d2h_bytes_per_step": N_QUERIES * 8,
-           "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 24) - 1) >> 24}
+    e2e = None if args.no_e2e else measure_e2e(t, q, out, stream, world, args)
 
     if not args.quick:
         extra.update(extra_measurements(t, keys, q, out, stream, args))
@@ -369,6 +370,28 @@ def run_gpu(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def measure_e2e(t, q, out, stream, world, args):
+    """Find through the C ABI with pinned HOST buffers: copy-in and copy-out
+    of every step are inside the timed region."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hq = q.cpu().pin_memory()
+    ho = torch.empty(N_QUERIES, dtype=torch.int64).pin_memory()
+    t.FindHost(hq.numpy(), ho.numpy())
+    torch.cuda.synchronize()
+    e2e_steps = max(3, min(args.steps, 10))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        t.FindHost(hq.numpy(), ho.numpy())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e2e_steps
+    assert torch.equal(ho, out.cpu()), "host-buffer Find differs from device Find"
+    return {"value": round(world * N_QUERIES / (e2e_ms / 1e3) / 1e9, 4), "unit": UNIT,
+            "h2d_bytes_per_step": N_QUERIES * 8, "d2h_bytes_per_step": N_QUERIES * 8,
+            "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 24) - 1) >> 24}
 
 
 def host_side_checks(t, q, out, args):
@@ -518,10 +541,17 @@ def main():
     ap.add_argument("--shape", default="", help="Find kernel shape LANESxITEMS, e.g. 8x1")
     ap.add_argument("--quick", action="store_true", help="skip the secondary measurements")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-host", action="store_true", help="skip the host-side oracle checks and CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end measurement")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--capacity-log2", type=int, default=28, help="requested capacity 2^k (profiling: smaller)")
+    ap.add_argument("--queries-log2", type=int, default=27, help="queries per step 2^k (profiling: smaller)")
+    ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("warmup must be >= 3")
+    global REQ_CAPACITY, N_QUERIES
+    REQ_CAPACITY, N_QUERIES = 1 << args.capacity_log2, 1 << args.queries_log2
     if args.impl == "reference":
         run_reference(args)
     else:

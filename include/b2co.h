@@ -58,6 +58,13 @@ const char* b2co_last_error(void);
 const char* b2co_status_string(int status);
 /* Library version string. */
 const char* b2co_version(void);
+/* Device wait policy (no reference counterpart).  Kernels that wait on their
+ * own asynchronous copies give up after `limit_ns` (0 = the default, 1 s),
+ * record it in the object's status word and return; the next synchronizing
+ * call on that object reports B2CO_ETIMEOUT.  `probe_timeout` != 0 is a test
+ * hook: the first wait of each block is made on a barrier that nothing ever
+ * arrives on, so the timeout path runs without any fault. */
+int b2co_debug_set_wait(uint64_t limit_ns, int probe_timeout);
 
 /* ===================================================================== */
 /* Open-addressing tables: StaticMap<K,T> and StaticSet<K>                 */

@@ -181,6 +181,16 @@ B2CO_HD uint32_t probe_next(uint32_t idx, uint32_t step, uint32_t capacity)
 // (pair.h:41, pair.inl:19-24), or a bare key for sets
 // ---------------------------------------------------------------------------
 
+// Device-side wait policy of kernels that wait on asynchronous copies: a wait
+// that exceeds `ns` nanoseconds stores kStatusTimeout into *status and the
+// kernel returns instead of waiting on.
+constexpr unsigned int kStatusTimeout = 1;
+struct WaitCtl {
+    unsigned int* status;
+    unsigned long long ns;
+    unsigned int probe_timeout;  // test hook: the first wait is on a barrier nothing arrives on
+};
+
 struct alignas(16) U128 {
     uint64_t lo, hi;
 };
@@ -263,6 +273,54 @@ __device__ __forceinline__ U128 ld_ro(U128 const* p)
     ulonglong2 v = __ldg(reinterpret_cast<ulonglong2 const*>(p));
     return U128{v.x, v.y};
 }
+// ---- bulk copies (TMA, untiled) and mbarriers --------------------------------
+__device__ __forceinline__ uint32_t smem_u32(void const* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Orders this thread's generic-proxy shared-memory accesses before later async-proxy (bulk copy) ones.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Global -> shared bulk copy completing on `bar`; dst, src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, void const* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for phase `parity` of `bar` for at most `limit_ns` nanoseconds.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    uint64_t const t0 = global_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_ns() - t0 > limit_ns) return false;
+    return true;
+}
+
 // Coherent loads for kernels that race with writers to the same table.
 __device__ __forceinline__ uint32_t ld_rw(uint32_t const* p) { return *reinterpret_cast<volatile uint32_t const*>(p); }
 __device__ __forceinline__ unsigned long long ld_rw(unsigned long long const* p)

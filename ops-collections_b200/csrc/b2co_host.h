@@ -35,7 +35,11 @@ uint32_t grid_for(void const* kernel, uint32_t block, uint64_t work, uint64_t pe
 // detail/open_addressing/open_addressing_impl.h:534-545).
 constexpr uint64_t kMaxBatch = (1ull << 32) - (1ull << 22);
 
-// Capacity prime rule (include/utility/prime.h:15 regenerated; see capacity.cpp).
+// Wait policy handed to kernels that wait on asynchronous copies (limit 1 s by
+// default; b2co_debug_set_wait changes it for tests).
+WaitCtl wait_ctl(unsigned int* status);
+
+// Capacity prime rule (include/utility/prime.h:15 regenerated; see runtime.cu).
 uint64_t prime_at_least(uint64_t n);
 uint64_t prime_table_last();
 
@@ -53,7 +57,7 @@ struct OaOps {
     int (*iaf_first)(OaArgs const& a, uint32_t b, void const* pairs, void* found, uint8_t* inserted, uint32_t n,
                      uint32_t* pos, uint32_t* newbits, uint32_t* owner, cudaStream_t s);
     int (*find)(OaArgs const& a, uint32_t b, uint32_t lanes, uint32_t items, bool contains, void const* keys,
-                uint8_t const* stencil, void* out, uint32_t n, cudaStream_t s);
+                uint8_t const* stencil, void* out, uint32_t n, WaitCtl wc, cudaStream_t s);
     int (*erase)(OaArgs const& a, uint32_t b, void const* keys, uint32_t n, unsigned long long* counters,
                  cudaStream_t s);
     int (*count)(OaArgs const& a, uint32_t b, void const* keys, uint32_t n, unsigned long long* counter,

@@ -71,24 +71,37 @@ cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 // Default lookup shape per layout; the autotuner overrides it per table.
 void default_shape(b2co_oa_table* t)
 {
-    uint32_t sb = slot_bytes(t->desc.key_bytes, t->desc.value_bytes);
     if (t->desc.bucket_size == 1) {
-        t->find_lanes = 1;
+        t->find_lanes = 1;  // a one-slot window needs no cooperation
         t->find_items = 4;
-    } else if (sb == 16) {
-        t->find_lanes = 1;
-        t->find_items = 2;
     } else {
-        t->find_lanes = 1;
-        t->find_items = 2;
+        t->find_lanes = 8;  // one slot per lane, staged keys, 4 windows per tile in flight
+        t->find_items = 4;
     }
 }
+
+unsigned int* status_word(b2co_oa_table* t) { return reinterpret_cast<unsigned int*>(t->d_counters + 2); }
 
 int launch_find(b2co_oa_table* t, bool contains, void const* keys, uint8_t const* stencil, void* out, uint64_t n,
                 cudaStream_t s)
 {
     return t->ops->find(t->args, t->desc.bucket_size, t->find_lanes, t->find_items, contains, keys, stencil, out,
-                        uint32_t(n), s);
+                        uint32_t(n), wait_ctl(status_word(t)), s);
+}
+
+// Reads (and clears) the table's device status word; a set word means a
+// bounded device wait expired in some earlier kernel on this table.
+int check_status(b2co_oa_table* t, cudaStream_t s)
+{
+    B2CO_CUDA(cudaMemcpyAsync(t->h_counters + 2, t->d_counters + 2, sizeof(unsigned long long),
+                              cudaMemcpyDeviceToHost, s));
+    B2CO_CUDA(cudaStreamSynchronize(s));
+    if (t->h_counters[2] != 0) {
+        B2CO_CUDA(cudaMemsetAsync(t->d_counters + 2, 0, sizeof(unsigned long long), s));
+        B2CO_CUDA(cudaStreamSynchronize(s));
+        return fail(B2CO_ETIMEOUT, "a bounded device wait expired (bulk key copy did not complete in time)");
+    }
+    return B2CO_OK;
 }
 
 int sync_counters(b2co_oa_table* t, cudaStream_t s, int words)
@@ -162,8 +175,10 @@ int b2co_oa_create_ex(b2co_oa_desc const* d, uint64_t requested, bool clear, b2c
     t->args.erased_key = t->desc.erased_key_bits;
 
     cudaError_t e = cudaMalloc(&t->args.slots, cap * slot_bytes(d->key_bytes, d->value_bytes));
-    if (e == cudaSuccess) e = cudaMalloc(&t->d_counters, 2 * sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMallocHost(&t->h_counters, 2 * sizeof(unsigned long long));
+    // counters: [failed, assigned, status word]
+    if (e == cudaSuccess) e = cudaMalloc(&t->d_counters, 3 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(t->d_counters, 0, 3 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMallocHost(&t->h_counters, 3 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         b2co_oa_destroy(t);
         return cuda_fail(e, "table allocation");
@@ -397,8 +412,7 @@ static int lookup_sync(b2co_oa_table* t, bool contains, void const* keys, uint8_
                        void* out, uint64_t n, b2co_stream s)
 {
     if (int st = lookup_async(t, contains, keys, stencil, use_stencil, out, n, s)) return st;
-    B2CO_CUDA(cudaStreamSynchronize(cs(s)));
-    return B2CO_OK;
+    return check_status(t, cs(s));
 }
 
 int b2co_oa_find(b2co_oa_table* t, void const* k, void* o, uint64_t n, b2co_stream s)
@@ -484,8 +498,7 @@ int b2co_oa_find_host(b2co_oa_table* t, void const* host_keys, void* host_out, u
         B2CO_CUDA(cudaEventRecord(t->ev[i], t->pipe[i]));
         B2CO_CUDA(cudaStreamWaitEvent(c, t->ev[i], 0));
     }
-    B2CO_CUDA(cudaStreamSynchronize(c));
-    return B2CO_OK;
+    return check_status(t, c);
 }
 
 }  // extern "C"

@@ -88,10 +88,32 @@ struct OaImpl {
         });
     }
 
+    template <int B, int G, bool C>
+    static int find_staged(OaArgs const& a, uint32_t items, void const* keys, void* out, uint32_t n, WaitCtl wc,
+                           cudaStream_t s)
+    {
+        void (*k)(OaArgs, void const*, void*, uint32_t, WaitCtl) = nullptr;
+        if (items >= 4 && G >= 4) k = k_find_staged<S, B, G, (G >= 4 ? 4 : 1), C>;
+        else if (items >= 2) k = k_find_staged<S, B, G, 2, C>;
+        else k = k_find_staged<S, B, G, 1, C>;
+        uint64_t chunks = n / kStageKeys;
+        uint32_t grid = grid_for((void const*)k, kBlock, chunks ? chunks : 1, 1);
+        k<<<grid, kBlock, 0, s>>>(a, keys, out, n, wc);
+        return check_launch(C ? "contains kernel" : "find kernel");
+    }
+
     template <int B, bool C>
     static int find_shape(OaArgs const& a, uint32_t lanes, uint32_t items, void const* keys, uint8_t const* stencil,
-                          void* out, uint32_t n, cudaStream_t s)
+                          void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
     {
+        // staged path: no stencil, 16-byte aligned key stream, at least one stage of keys
+        bool const staged = !stencil && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 && n >= kStageKeys && B > 1 &&
+                            lanes >= 2;
+        if (staged) {
+            if (lanes == 2) return find_staged<B, 2, C>(a, items, keys, out, n, wc, s);
+            if (lanes == 4) return find_staged<B, 4, C>(a, items, keys, out, n, wc, s);
+            return find_staged<B, 8, C>(a, items, keys, out, n, wc, s);
+        }
         void (*k)(OaArgs, void const*, uint8_t const*, void*, uint32_t) = nullptr;
         uint64_t per_block = kBlock;
         if (B == 1 || lanes <= 1) {
@@ -110,12 +132,12 @@ struct OaImpl {
     }
 
     static int find(OaArgs const& a, uint32_t b, uint32_t lanes, uint32_t items, bool contains, void const* keys,
-                    uint8_t const* stencil, void* out, uint32_t n, cudaStream_t s)
+                    uint8_t const* stencil, void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
     {
         return with_b(b, [&](auto bc) {
             constexpr int B = decltype(bc)::value;
-            return contains ? find_shape<B, true>(a, lanes, items, keys, stencil, out, n, s)
-                            : find_shape<B, false>(a, lanes, items, keys, stencil, out, n, s);
+            return contains ? find_shape<B, true>(a, lanes, items, keys, stencil, out, n, wc, s)
+                            : find_shape<B, false>(a, lanes, items, keys, stencil, out, n, wc, s);
         });
     }
 

@@ -179,7 +179,9 @@ __global__ void __launch_bounds__(256) k_insert(OaArgs a, void const* pairs, uin
         if (i < n && (!stencil || stencil[i])) {
             typename S::Raw p = Io<S>::load_pair(pairs, i);
             int r = insert_one<S, B, ASSIGN>(a, S::key(p), S::value(p));
-            failed += r == kFailed;
+            // Insert succeeds only on SUCCESS (open_addressing_ref_impl.h:282-285), so a
+            // duplicate is a failure; InsertOrAssign counts it as an assignment instead.
+            failed += ASSIGN ? r == kFailed : r != kSuccess;
             assigned += r == kDuplicate;
         }
     }
@@ -417,7 +419,7 @@ __device__ __noinline__ bool find_rest(OaArgs const& a, uint64_t key, uint32_t i
         load_window<S, B>(slots, idx, w);
         int j = scan_window<S, B>(w, key, a.empty_key);
         if (j >= 0) {
-            bool hit = S::key(w[j]) == key;
+            bool hit = S::key(w[j]) != a.empty_key;  // an empty slot ends the scan first
             payload = hit ? S::value(w[j]) : empty_payload<S>(a);
             return hit;
         }
@@ -460,7 +462,7 @@ __global__ void __launch_bounds__(256) k_find_lane(OaArgs a, void const* keys, u
             if (live[t]) {
                 int j = scan_window<S, B>(w[t], key[t], a.empty_key);
                 if (j >= 0) {
-                    hit = S::key(w[t][j]) == key[t];
+                    hit = S::key(w[t][j]) != a.empty_key;
                     if (hit) payload = S::value(w[t][j]);
                 } else {
                     hit = find_rest<S, B>(a, key[t], init[t], payload);
@@ -507,7 +509,7 @@ __global__ void __launch_bounds__(256) k_find_tile(OaArgs a, void const* keys, u
                     w[t] = ld_ro(slots + idx + j);
                     k = S::key(w[t]);
                 }
-                bool is_hit = own && k == key;
+                bool is_hit = own && k == key && k != a.empty_key;
                 bool is_stop = own && (k == a.empty_key || is_hit);
                 stop_bits |= ((__ballot_sync(0xffffffffu, is_stop) >> tile_shift) & TILE_MASK) << (t * G);
                 hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> tile_shift) & TILE_MASK) << (t * G);
@@ -534,6 +536,204 @@ __global__ void __launch_bounds__(256) k_find_tile(OaArgs a, void const* keys, u
         if (r == 0 && i < n) {
             if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = hit;
             else Io<S>::store_payload(out, i, hit ? pv : empty_payload<S>(a));
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Staged lookups: the key stream is brought into shared memory by bulk (TMA)
+// copies, double-buffered, one 1024-key chunk per stage, so no lane waits on a
+// key load before it can probe.  G lanes cooperate on a bucket window (one
+// 16-byte slot per lane and round); each tile keeps Q windows in flight; the
+// probe start index is hashed once per key (lane q of the tile) and shuffled.
+// Keys of a pass are interleaved across tiles, so the tiles' first lanes
+// store consecutive outputs.
+// ----------------------------------------------------------------------------
+
+constexpr uint32_t kStageKeys = 1024;
+
+struct TileResult {
+    uint64_t payload;
+    bool hit;
+    bool done;
+};
+
+// Resolves one loaded window of a tile (the whole warp calls it; tiles with
+// `skip` set only take part in the ballots).  When the window ends the scan,
+// the result has done set, the hit flag, and -- on every lane of the tile --
+// the payload of the hit slot, handed over by the lane that loaded it.
+template <class S, int B, int G, int ROUNDS>
+__device__ __forceinline__ void tile_resolve(OaArgs const& a, typename S::Raw const (&w)[ROUNDS], uint64_t key,
+                                             uint32_t r, uint32_t lane0, bool skip, TileResult& res)
+{
+    constexpr uint32_t MASK = (1u << G) - 1u;
+    uint32_t stop_bits = 0, hit_bits = 0;
+#pragma unroll
+    for (int t = 0; t < ROUNDS; ++t) {
+        bool const own = !skip && int(r) + t * G < B;
+        uint64_t const k = own ? S::key(w[t]) : 0;
+        bool const is_stop = own && (k == a.empty_key || k == key);
+        bool const is_hit = is_stop && k != a.empty_key;
+        stop_bits |= ((__ballot_sync(0xffffffffu, is_stop) >> lane0) & MASK) << (t * G);
+        hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> lane0) & MASK) << (t * G);
+    }
+    int const stop_j = stop_bits ? __ffs(stop_bits) - 1 : -1;
+    uint64_t mine = 0;
+    if (stop_j >= 0 && int(r) == stop_j % G) {
+#pragma unroll
+        for (int t = 0; t < ROUNDS; ++t)
+            if (t == stop_j / G) mine = S::value(w[t]);
+    }
+    uint64_t const got = __shfl_sync(0xffffffffu, (unsigned long long)mine, lane0 + (stop_j >= 0 ? stop_j % G : 0));
+    if (!skip && stop_j >= 0) {
+        res.done = true;
+        res.hit = (hit_bits >> stop_j) & 1u;
+        res.payload = got;
+    }
+}
+
+// Further windows of keys whose first window neither held the key nor an
+// empty slot (rare at load factor 0.5); the whole warp iterates until every
+// tile is done.
+template <class S, int B, int G, int ROUNDS>
+__device__ __noinline__ TileResult tile_continue(OaArgs a, typename S::Raw const* slots, uint64_t key, uint32_t init,
+                                                 uint32_t r, uint32_t lane0, TileResult res)
+{
+    uint32_t idx = init, step = 0;
+    while (__any_sync(0xffffffffu, !res.done)) {
+        typename S::Raw w[ROUNDS];
+        if (!res.done) {
+            if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
+            idx = probe_next(idx, step, a.probe.capacity);
+            if (idx == init) {
+                res.done = true;  // full cycle: not present
+                res.hit = false;
+            } else {
+#pragma unroll
+                for (int t = 0; t < ROUNDS; ++t)
+                    if (int(r) + t * G < B) w[t] = ld_ro(slots + idx + r + t * G);
+            }
+        }
+        tile_resolve<S, B, G, ROUNDS>(a, w, key, r, lane0, res.done, res);
+    }
+    return res;
+}
+
+template <class S, int B, int G, int Q, bool CONTAINS>
+__global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
+{
+    static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");
+    using Raw = typename S::Raw;
+    using Key = typename Io<S>::Key;
+    constexpr int ROUNDS = (B + G - 1) / G;
+    constexpr uint32_t TILES = 256 / G;             // tiles per block
+    constexpr uint32_t PASS = TILES * Q;            // keys per pass
+    static_assert(kStageKeys % PASS == 0, "stage must hold whole passes");
+    __shared__ alignas(128) Key sk[2][kStageKeys];
+    __shared__ alignas(8) uint64_t bar[2];
+    __shared__ alignas(8) uint64_t never;  // no thread or copy ever arrives on it (timeout test hook)
+
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t const lane = threadIdx.x & 31, r = lane % G, tile_lane0 = lane & ~uint32_t(G - 1);
+    uint32_t const tile = threadIdx.x / G;
+    uint32_t const chunks = n / kStageKeys;
+    constexpr uint32_t kChunkBytes = kStageKeys * sizeof(Key);
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init(&never, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && blockIdx.x < chunks) {
+        mbar_arrive_expect_tx(&bar[0], kChunkBytes);
+        bulk_g2s(sk[0], static_cast<Key const*>(keys) + uint64_t(blockIdx.x) * kStageKeys, kChunkBytes, &bar[0]);
+    }
+    uint32_t it = 0;
+    bool failed = false;
+    for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x, ++it) {
+        uint32_t const b = it & 1;
+        uint32_t const cn = c + gridDim.x;
+        if (threadIdx.x == 0 && cn < chunks) {
+            fence_proxy_async();  // the other buffer's generic reads (previous chunk) precede this copy
+            mbar_arrive_expect_tx(&bar[b ^ 1], kChunkBytes);
+            bulk_g2s(sk[b ^ 1], static_cast<Key const*>(keys) + uint64_t(cn) * kStageKeys, kChunkBytes, &bar[b ^ 1]);
+        }
+        // the whole block agrees on the outcome, so every lane leaves together
+        bool const ok = wc.probe_timeout ? mbar_wait_bounded(&never, 0, wc.ns)
+                                         : mbar_wait_bounded(&bar[b], (it >> 1) & 1, wc.ns);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        Key const* ks = sk[b];
+        uint32_t const base = c * kStageKeys;
+        for (uint32_t p = 0; p < kStageKeys; p += PASS) {
+            // key q of this tile sits at p + q * TILES + tile
+            uint64_t key[Q];
+            uint32_t idx[Q], init[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) key[q] = ks[p + q * TILES + tile];
+            uint32_t my_init = 0;
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                if (int(r) == q) my_init = probe_init<S::key_bytes, B>(a.probe, key[q]);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) idx[q] = init[q] = __shfl_sync(0xffffffffu, my_init, tile_lane0 + q);
+            // all Q first windows in flight before any is resolved
+            Raw w[Q][ROUNDS];
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int t = 0; t < ROUNDS; ++t)
+                    if (int(r) + t * G < B) w[q][t] = ld_ro(slots + idx[q] + r + t * G);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                TileResult res{0, false, false};
+                tile_resolve<S, B, G, ROUNDS>(a, w[q], key[q], r, tile_lane0, false, res);
+                if (__any_sync(0xffffffffu, !res.done))  // rare: some tile needs further windows
+                    res = tile_continue<S, B, G, ROUNDS>(a, slots, key[q], init[q], r, tile_lane0, res);
+                if (r == 0) {
+                    uint32_t const i = base + p + q * TILES + tile;
+                    if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = res.hit;
+                    else Io<S>::store_payload(out, i, res.hit ? res.payload : empty_payload<S>(a));
+                }
+            }
+        }
+        __syncthreads();  // every lane is done with sk[b] before it is refilled
+    }
+    if (failed) {
+        if (threadIdx.x == 0) {
+            atomicExch(wc.status, kStatusTimeout);
+            // let the copies still in flight land before the block exits (bounded again)
+            uint32_t const c = blockIdx.x + it * gridDim.x;
+            mbar_wait_bounded(&bar[it & 1], (it >> 1) & 1, 1000000000ull);
+            if (c + gridDim.x < chunks) mbar_wait_bounded(&bar[(it + 1) & 1], ((it + 1) >> 1) & 1, 1000000000ull);
+        }
+        return;
+    }
+    // the ragged tail (< one stage) goes through direct loads, block 0 only
+    if (blockIdx.x == 0 && chunks * kStageKeys < n) {
+        for (uint32_t i0 = chunks * kStageKeys; i0 < n; i0 += TILES) {
+            uint32_t const i = i0 + tile;
+            bool const live = i < n;
+            uint64_t const key = live ? Io<S>::load_key(keys, i) : 0;
+            uint32_t const init0 = live ? probe_init<S::key_bytes, B>(a.probe, key) : 0;
+            Raw w[ROUNDS];
+            if (live) {
+#pragma unroll
+                for (int t = 0; t < ROUNDS; ++t)
+                    if (int(r) + t * G < B) w[t] = ld_ro(slots + init0 + r + t * G);
+            }
+            TileResult res{0, false, !live};
+            tile_resolve<S, B, G, ROUNDS>(a, w, key, r, tile_lane0, !live, res);
+            if (__any_sync(0xffffffffu, !res.done))
+                res = tile_continue<S, B, G, ROUNDS>(a, slots, key, init0, r, tile_lane0, res);
+            if (r == 0 && live) {
+                if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = res.hit;
+                else Io<S>::store_payload(out, i, res.hit ? res.payload : empty_payload<S>(a));
+            }
         }
     }
 }
@@ -609,7 +809,7 @@ __global__ void __launch_bounds__(256) k_count(OaArgs a, void const* keys, uint3
         load_window<S, B>(slots, init, w);
         int j = scan_window<S, B>(w, key, a.empty_key);
         uint64_t payload;
-        if (j >= 0) c += S::key(w[j]) == key;
+        if (j >= 0) c += S::key(w[j]) != a.empty_key;
         else c += find_rest<S, B>(a, key, init, payload);
     }
     warp_add_counter(counter, c);

@@ -1,5 +1,6 @@
 // runtime.cu -- error state, launch geometry and the capacity prime rule.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -59,6 +60,11 @@ uint32_t grid_for(void const* kernel, uint32_t block, uint64_t work, uint64_t pe
     if (want < 1) want = 1;
     return uint32_t(want < cap ? want : cap);
 }
+
+static std::atomic<unsigned long long> g_wait_ns{1000000000ull};
+static std::atomic<unsigned int> g_wait_probe{0};
+
+WaitCtl wait_ctl(unsigned int* status) { return WaitCtl{status, g_wait_ns.load(), g_wait_probe.load()}; }
 
 // ---------------------------------------------------------------------------
 // Capacity primes.  The reference's table (include/utility/prime.h:15, 140,741
@@ -156,6 +162,13 @@ const char* b2co_status_string(int s)
 }
 
 const char* b2co_version(void) { return "b2co 0.1 (sm_100a)"; }
+
+int b2co_debug_set_wait(uint64_t limit_ns, int probe_timeout)
+{
+    b2co::g_wait_ns.store(limit_ns ? limit_ns : 1000000000ull);
+    b2co::g_wait_probe.store(probe_timeout ? 1u : 0u);
+    return B2CO_OK;
+}
 
 // MakeValidExtent (include/detail/extent/extent.inl:20-62).
 int b2co_oa_valid_capacity(uint64_t requested, uint32_t b, uint32_t probing, uint64_t* capacity)

@@ -14,13 +14,19 @@ def torch_dt(nbytes):
 
 
 def unique_keys(rng, n, kb, lo=0, hi=None):
-    """n distinct keys, never the -1 sentinel (generators.h style: uniform draws)."""
-    hi = hi if hi is not None else (2**31 - 2 if kb == 4 else 2**62)
+    """n distinct keys, never the -1 sentinel (generators.h style: uniform draws).
+    The default range [0, 2^30) (4-byte) / [0, 2^62) (8-byte) never meets miss_keys()."""
+    hi = hi if hi is not None else (2**30 if kb == 4 else 2**62)
     out = np.unique(rng.integers(lo, hi, size=int(n * 1.3) + 16, dtype=np.int64))
     rng.shuffle(out)
     out = out[:n]
     assert len(out) == n
     return out.astype(NP_DT[kb])
+
+
+def miss_keys(rng, n, kb):
+    """n distinct keys from a range disjoint from unique_keys()' default range."""
+    return unique_keys(rng, n, kb, lo=2**30 if kb == 4 else 2**62, hi=2**31 - 2 if kb == 4 else 2**63 - 2)
 
 
 def dev(a):

@@ -5,7 +5,7 @@ against a host dictionary golden (tests/common/golden.h)."""
 import numpy as np
 import pytest
 
-from helpers import dev, unique_keys
+from helpers import dev, miss_keys, unique_keys
 
 pytestmark = pytest.mark.gpu
 
@@ -41,7 +41,7 @@ def test_dynamic_map_growth_find_erase(kb, vb):
         off += size
     assert m.Size() == len(gold)
     assert m.NumSubmaps() > 1
-    q = np.concatenate([keys, unique_keys(rng, 20000, kb, lo=2**30 if kb == 4 else 2**62)])
+    q = np.concatenate([keys, miss_keys(rng, 20000, kb)])
     out = torch.empty(len(q), dtype=tdt[vb], device="cuda")
     m.Find(dev(q), out)
     exp = np.array([gold.get(int(x), -1) for x in q], dtype=kdt[vb])

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from helpers import LAYOUTS, NP_DT, dev, make_pairs, oracle_table, stored_pairs, torch_dt, unique_keys
+from helpers import LAYOUTS, NP_DT, dev, make_pairs, miss_keys, oracle_table, stored_pairs, torch_dt, unique_keys
 
 pytestmark = pytest.mark.gpu
 
@@ -205,7 +205,7 @@ def test_erase_parity(layout, tombstone):
     # Later lookups depend on where erased slots sit in probe sequences, so
     # erase from identical slot positions: the oracle takes the device layout.
     o.load_slots(t.dump_slots())
-    gone = np.concatenate([keys[:3000], unique_keys(rng, 500, kb, lo=2**30 if kb == 4 else 2**62)])
+    gone = np.concatenate([keys[:3000], miss_keys(rng, 500, kb)])
     assert t.Erase(dev(gone)) == o.erase(gone) == 500
     q = np.concatenate([keys, gone])
     out = out_buf(len(q), kb, vb)
@@ -231,7 +231,7 @@ def test_full_table(layout):
     c = torch.empty(len(keys), dtype=torch.uint8, device="cuda")
     t.Contains(dev(keys), c)
     assert int(c.sum()) == cap
-    assert t.Count(dev(unique_keys(rng, 50, kb, lo=2**30 if kb == 4 else 2**62))) == 0
+    assert t.Count(dev(miss_keys(rng, 50, kb))) == 0
 
 
 def test_edge_cases_and_errors():
@@ -264,7 +264,7 @@ def test_find_shapes_agree():
         keys = unique_keys(rng, 200000, kb)   # high load: many second windows
         vals = values_for(rng, keys, vb)
         t.Insert(make_pairs(keys, vals))
-        q = np.concatenate([keys[::3], unique_keys(rng, 50000, kb, lo=2**30 if kb == 4 else 2**62)])
+        q = np.concatenate([keys[::3], miss_keys(rng, 50000, kb)])
         qd = dev(q)
         ref = None
         for lanes in (1, 2, 4, 8):
@@ -287,7 +287,7 @@ def test_find_host_buffers_match_device_find():
     keys = unique_keys(rng, 1 << 19, 8)
     vals = values_for(rng, keys, 8)
     t.Insert(make_pairs(keys, vals))
-    q = np.concatenate([keys, unique_keys(rng, 1 << 19, 8, lo=2**62)])
+    q = np.concatenate([keys, miss_keys(rng, 1 << 19, 8)])
     rng.shuffle(q)
     pinned_q = torch.from_numpy(q).pin_memory()
     pinned_o = torch.empty(len(q), dtype=torch.int64).pin_memory()
