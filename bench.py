@@ -211,6 +211,13 @@ class ClockSampler:
 # helpers
 # ---------------------------------------------------------------------------
 
+def parse_shape(s: str):
+    """'LxK' or 'LxKs': L lanes per key, K keys in flight per lane group, s = segmented windows."""
+    seg = s.endswith("s")
+    lanes, items = (int(x) for x in s.rstrip("s").split("x"))
+    return lanes, items, seg
+
+
 def peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -297,8 +304,9 @@ def run_gpu(args):
     out = torch.empty(N_QUERIES, dtype=torch.int64, device="cuda")
     if args.sweep:
         sweep = {}
-        for lanes, items in [(1, 2), (1, 4), (2, 2), (4, 1), (4, 2), (4, 4), (8, 1), (8, 2), (8, 4)]:
-            t.set_find_shape(lanes, items)
+        for shape in ["1x4", "2x2", "4x2", "4x4", "8x4", "2x2s", "4x1s", "4x2s", "4x4s", "8x2s", "8x4s"]:
+            lanes, items, seg = parse_shape(shape)
+            t.set_find_shape(lanes, items, seg)
             for _ in range(3):
                 t.FindAsync(q, out)
             torch.cuda.synchronize()
@@ -307,12 +315,11 @@ def run_gpu(args):
                 t.FindAsync(q, out)
             e1.record(stream)
             torch.cuda.synchronize()
-            sweep[f"{lanes}x{items}"] = round(N_QUERIES * 10 / e0.elapsed_time(e1) / 1e6, 3)
-            log(f"[sweep] lanes {lanes} items {items}: {sweep[f'{lanes}x{items}']} Gkeys/s")
+            sweep[shape] = round(N_QUERIES * 10 / e0.elapsed_time(e1) / 1e6, 3)
+            log(f"[sweep] shape {shape}: {sweep[shape]} Gkeys/s")
         t.set_find_shape(0, 0)
     if args.shape:
-        lanes, items = (int(x) for x in args.shape.split("x"))
-        t.set_find_shape(lanes, items)
+        t.set_find_shape(*parse_shape(args.shape))
 
     for _ in range(args.warmup):
         t.FindAsync(q, out)

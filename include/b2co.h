@@ -163,9 +163,12 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
                       b2co_stream stream);
 
 /* Kernel shape used by Find/Contains on this table: lanes per key (1, 2, 4 or
- * 8) and keys per lane per pass (1, 2 or 4); 0 = library default.  The
- * autotuner sets these.  No reference counterpart (the reference launches one
- * thread per key). */
+ * 8) and keys in flight per lane group (1, 2 or 4), optionally OR-ed with
+ * B2CO_FIND_SEGMENTED (scan each first bucket window by 64-byte segments and
+ * read the second segment only when the first does not end the scan); 0, 0 =
+ * library default.  The autotuner sets these.  No reference counterpart (the
+ * reference launches one thread per key). */
+#define B2CO_FIND_SEGMENTED 0x100u
 int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_lane);
 
 /* ===================================================================== */

@@ -45,6 +45,10 @@ uint64_t prime_table_last();
 
 struct OaArgs;
 
+// Lookup shape flag carried in the keys-per-lane field: scan each first window
+// by 64-byte segments (B2CO_FIND_SEGMENTED in the C ABI).
+constexpr uint32_t kShapeSegmented = 0x100;
+
 // Launchers for one slot layout; B (bucket size) is dispatched at run time.
 struct OaOps {
     int (*clear)(OaArgs const& a, cudaStream_t s);

@@ -88,14 +88,14 @@ struct OaImpl {
         });
     }
 
-    template <int B, int G, bool C>
+    template <int B, int G, bool C, bool SEG>
     static int find_staged(OaArgs const& a, uint32_t items, void const* keys, void* out, uint32_t n, WaitCtl wc,
                            cudaStream_t s)
     {
         void (*k)(OaArgs, void const*, void*, uint32_t, WaitCtl) = nullptr;
-        if (items >= 4 && G >= 4) k = k_find_staged<S, B, G, (G >= 4 ? 4 : 1), C>;
-        else if (items >= 2) k = k_find_staged<S, B, G, 2, C>;
-        else k = k_find_staged<S, B, G, 1, C>;
+        if (items >= 4 && G >= 4) k = k_find_staged<S, B, G, (G >= 4 ? 4 : 1), C, SEG>;
+        else if (items >= 2) k = k_find_staged<S, B, G, 2, C, SEG>;
+        else k = k_find_staged<S, B, G, 1, C, SEG>;
         uint64_t chunks = n / kStageKeys;
         uint32_t grid = grid_for((void const*)k, kBlock, chunks ? chunks : 1, 1);
         k<<<grid, kBlock, 0, s>>>(a, keys, out, n, wc);
@@ -110,10 +110,18 @@ struct OaImpl {
         bool const staged = !stencil && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 && n >= kStageKeys && B > 1 &&
                             lanes >= 2;
         if (staged) {
-            if (lanes == 2) return find_staged<B, 2, C>(a, items, keys, out, n, wc, s);
-            if (lanes == 4) return find_staged<B, 4, C>(a, items, keys, out, n, wc, s);
-            return find_staged<B, 8, C>(a, items, keys, out, n, wc, s);
+            bool const seg = (items & kShapeSegmented) != 0;
+            items &= ~kShapeSegmented;
+            if (seg) {
+                if (lanes == 2) return find_staged<B, 2, C, true>(a, items, keys, out, n, wc, s);
+                if (lanes == 4) return find_staged<B, 4, C, true>(a, items, keys, out, n, wc, s);
+                return find_staged<B, 8, C, true>(a, items, keys, out, n, wc, s);
+            }
+            if (lanes == 2) return find_staged<B, 2, C, false>(a, items, keys, out, n, wc, s);
+            if (lanes == 4) return find_staged<B, 4, C, false>(a, items, keys, out, n, wc, s);
+            return find_staged<B, 8, C, false>(a, items, keys, out, n, wc, s);
         }
+        items &= ~kShapeSegmented;
         void (*k)(OaArgs, void const*, uint8_t const*, void*, uint32_t) = nullptr;
         uint64_t per_block = kBlock;
         if (B == 1 || lanes <= 1) {

@@ -592,6 +592,55 @@ __device__ __forceinline__ void tile_resolve(OaArgs const& a, typename S::Raw co
     }
 }
 
+// Segment-wise scan of one window: slots [lo, hi) of the window starting at
+// slot `idx`, loaded one slot per lane (at most G slots per call).  DRAM serves
+// random reads in 64-byte bursts, and an 80-byte bucket always spans two, so
+// the first call covers only the slots up to the next 64-byte boundary and the
+// second runs only for tiles whose first segment neither held the key nor an
+// empty slot.
+template <class S, int G>
+__device__ __forceinline__ void resolve_segment(OaArgs const& a, typename S::Raw w, bool own, uint64_t key, uint32_t r,
+                                                uint32_t lane0, bool skip, TileResult& res)
+{
+    constexpr uint32_t MASK = (1u << G) - 1u;
+    own = own && !skip;
+    uint64_t const k = own ? S::key(w) : 0;
+    bool const is_stop = own && (k == a.empty_key || k == key);
+    bool const is_hit = is_stop && k != a.empty_key;
+    uint32_t const stop_bits = (__ballot_sync(0xffffffffu, is_stop) >> lane0) & MASK;
+    uint32_t const hit_bits = (__ballot_sync(0xffffffffu, is_hit) >> lane0) & MASK;
+    int const s = stop_bits ? __ffs(stop_bits) - 1 : -1;
+    uint64_t const mine = (s >= 0 && int(r) == s) ? S::value(w) : 0;
+    uint64_t const got = __shfl_sync(0xffffffffu, (unsigned long long)mine, lane0 + (s >= 0 ? s : 0));
+    if (!skip && s >= 0) {
+        res.done = true;
+        res.hit = (hit_bits >> s) & 1u;
+        res.payload = got;
+    }
+}
+
+// End of the segment that starts at window slot `lo`: the next 64-byte
+// boundary, the window's end, or G slots further, whichever comes first.
+template <class S, int B, int G>
+__device__ __forceinline__ int segment_end(uint32_t idx, int lo)
+{
+    constexpr int per = 64 / S::bytes;
+    int hi = lo + per - int((idx + lo) % per);
+    if (hi > lo + G) hi = lo + G;
+    return hi < B ? hi : B;
+}
+
+template <class S, int B, int G>
+__device__ __forceinline__ void tile_segment(OaArgs const& a, typename S::Raw const* slots, uint32_t idx, int lo,
+                                             int hi, uint64_t key, uint32_t r, uint32_t lane0, bool skip,
+                                             TileResult& res)
+{
+    bool const own = !skip && lo + int(r) < hi;
+    typename S::Raw w{};
+    if (own) w = ld_ro(slots + idx + lo + r);
+    resolve_segment<S, G>(a, w, own, key, r, lane0, skip, res);
+}
+
 // Further windows of keys whose first window neither held the key nor an
 // empty slot (rare at load factor 0.5); the whole warp iterates until every
 // tile is done.
@@ -619,7 +668,7 @@ __device__ __noinline__ TileResult tile_continue(OaArgs a, typename S::Raw const
     return res;
 }
 
-template <class S, int B, int G, int Q, bool CONTAINS>
+template <class S, int B, int G, int Q, bool CONTAINS, bool SEG>
 __global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
 {
     static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");
@@ -681,6 +730,57 @@ __global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys,
                 if (int(r) == q) my_init = probe_init<S::key_bytes, B>(a.probe, key[q]);
 #pragma unroll
             for (int q = 0; q < Q; ++q) idx[q] = init[q] = __shfl_sync(0xffffffffu, my_init, tile_lane0 + q);
+            if constexpr (SEG) {
+                // first segment of every key's first window in flight together
+                Raw w1[Q];
+                int hi1[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    hi1[q] = segment_end<S, B, G>(idx[q], 0);
+                    w1[q] = Raw{};
+                    if (int(r) < hi1[q]) w1[q] = ld_ro(slots + idx[q] + r);
+                }
+                TileResult res[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    res[q] = TileResult{0, false, false};
+                    resolve_segment<S, G>(a, w1[q], int(r) < hi1[q], key[q], r, tile_lane0, false, res[q]);
+                }
+                // second segment only where the first did not end the scan, again all in flight
+                Raw w2[Q];
+                int lo2[Q], hi2[Q];
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    lo2[q] = hi1[q];
+                    bool const act = !res[q].done && lo2[q] < B;
+                    hi2[q] = act ? segment_end<S, B, G>(idx[q], lo2[q]) : lo2[q];
+                    w2[q] = Raw{};
+                    if (act && lo2[q] + int(r) < hi2[q]) w2[q] = ld_ro(slots + idx[q] + lo2[q] + r);
+                }
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
+                    if (__any_sync(0xffffffffu, !res[q].done && lo2[q] < B)) {
+                        bool const act = !res[q].done && lo2[q] < B;
+                        resolve_segment<S, G>(a, w2[q], act && lo2[q] + int(r) < hi2[q], key[q], r, tile_lane0, !act,
+                                              res[q]);
+                        int lo = hi2[q];
+                        while (__any_sync(0xffffffffu, !res[q].done && lo < B)) {  // windows wider than two segments
+                            bool const more = !res[q].done && lo < B;
+                            int const hi = more ? segment_end<S, B, G>(idx[q], lo) : lo;
+                            tile_segment<S, B, G>(a, slots, idx[q], lo, hi, key[q], r, tile_lane0, !more, res[q]);
+                            lo = hi;
+                        }
+                    }
+                    if (__any_sync(0xffffffffu, !res[q].done))  // rare: further windows
+                        res[q] = tile_continue<S, B, G, ROUNDS>(a, slots, key[q], init[q], r, tile_lane0, res[q]);
+                    if (r == 0) {
+                        uint32_t const i = base + p + q * TILES + tile;
+                        if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = res[q].hit;
+                        else Io<S>::store_payload(out, i, res[q].hit ? res[q].payload : empty_payload<S>(a));
+                    }
+                }
+                continue;
+            }
             // all Q first windows in flight before any is resolved
             Raw w[Q][ROUNDS];
 #pragma unroll

@@ -266,18 +266,19 @@ def test_find_shapes_agree():
         t.Insert(make_pairs(keys, vals))
         q = np.concatenate([keys[::3], miss_keys(rng, 50000, kb)])
         qd = dev(q)
-        ref = None
-        for lanes in (1, 2, 4, 8):
-            for items in (1, 2, 4):
-                t.set_find_shape(lanes, items)
-                out = out_buf(len(q), kb, vb)
-                t.Find(qd, out)
-                c = torch.empty(len(q), dtype=torch.uint8, device="cuda")
-                t.Contains(qd, c)
-                cur = (out.cpu().numpy(), c.cpu().numpy())
-                if ref is None:
-                    ref = cur
-                assert np.array_equal(cur[0], ref[0]) and np.array_equal(cur[1], ref[1]), (kb, vb, b, lanes, items)
+        o = oracle_table(t, kb, vb, b, oracle.PROBE_DOUBLE, oracle.HASH_XXH32)
+        o.insert(keys, vals)
+        ref = (o.find(q)[0], o.contains(q)[0])
+        shapes = [(l, i, False) for l in (1, 2, 4, 8) for i in (1, 2, 4)] + \
+                 [(l, i, True) for l in (2, 4, 8) for i in (1, 2, 4)]
+        for lanes, items, seg in shapes:
+            t.set_find_shape(lanes, items, seg)
+            out = out_buf(len(q), kb, vb)
+            t.Find(qd, out)
+            c = torch.empty(len(q), dtype=torch.uint8, device="cuda")
+            t.Contains(qd, c)
+            assert np.array_equal(out.cpu().numpy(), ref[0]), (kb, vb, b, lanes, items, seg)
+            assert np.array_equal(c.cpu().numpy(), ref[1]), (kb, vb, b, lanes, items, seg)
 
 
 def test_find_host_buffers_match_device_find():
