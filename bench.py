@@ -212,10 +212,13 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 
 def parse_shape(s: str):
-    """'LxK' or 'LxKs': L lanes per key, K keys in flight per lane group, s = segmented windows."""
+    """'LxK', 'LxKs' or 'bulk': L lanes per key, K keys in flight per lane group,
+    s = segmented windows, bulk = one bulk copy per bucket window."""
+    if s == "bulk":
+        return 1, 1, False, True
     seg = s.endswith("s")
     lanes, items = (int(x) for x in s.rstrip("s").split("x"))
-    return lanes, items, seg
+    return lanes, items, seg, False
 
 
 def peaks():
@@ -304,9 +307,8 @@ def run_gpu(args):
     out = torch.empty(N_QUERIES, dtype=torch.int64, device="cuda")
     if args.sweep:
         sweep = {}
-        for shape in ["1x4", "2x2", "4x2", "4x4", "8x4", "2x2s", "4x1s", "4x2s", "4x4s", "8x2s", "8x4s"]:
-            lanes, items, seg = parse_shape(shape)
-            t.set_find_shape(lanes, items, seg)
+        for shape in ["bulk", "2x2", "2x1", "4x1", "4x2", "8x4", "1x4"]:
+            t.set_find_shape(*parse_shape(shape))
             for _ in range(3):
                 t.FindAsync(q, out)
             torch.cuda.synchronize()

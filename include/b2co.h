@@ -169,6 +169,9 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
  * library default.  The autotuner sets these.  No reference counterpart (the
  * reference launches one thread per key). */
 #define B2CO_FIND_SEGMENTED 0x100u
+/* OR-ed into keys_per_lane: fetch every first bucket window with one bulk (TMA)
+ * copy into shared memory; tables with 16-byte slots only (others ignore it). */
+#define B2CO_FIND_BULK 0x200u
 int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_lane);
 
 /* ===================================================================== */

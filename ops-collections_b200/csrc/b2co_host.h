@@ -48,6 +48,9 @@ struct OaArgs;
 // Lookup shape flag carried in the keys-per-lane field: scan each first window
 // by 64-byte segments (B2CO_FIND_SEGMENTED in the C ABI).
 constexpr uint32_t kShapeSegmented = 0x100;
+// Lookup shape flag: fetch every first bucket window with one bulk (TMA) copy
+// into shared memory (16-byte slots; B2CO_FIND_BULK in the C ABI).
+constexpr uint32_t kShapeBulk = 0x200;
 
 // Launchers for one slot layout; B (bucket size) is dispatched at run time.
 struct OaOps {

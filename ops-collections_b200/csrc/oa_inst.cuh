@@ -103,12 +103,40 @@ struct OaImpl {
     }
 
     template <int B, bool C>
+    static int find_bulk(OaArgs const& a, void const* keys, void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
+    {
+        if constexpr (S::bytes == 16) {
+            auto k = k_find_bulk<S, B, C>;
+            constexpr uint32_t smem = bulk_window_smem<S, B>();
+            static bool attr = false;  // per instantiation
+            if (!attr) {
+                cudaError_t e = cudaFuncSetAttribute((void const*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+                if (e != cudaSuccess) return cuda_fail(e, "bulk find attribute");
+                attr = true;
+            }
+            int per_sm = 0;
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)k, kBlock, smem);
+            if (e != cudaSuccess) return cuda_fail(e, "bulk find occupancy");
+            uint64_t chunks = n / kStageKeys;
+            uint64_t cap = uint64_t(per_sm < 1 ? 1 : per_sm) * sm_count();
+            uint32_t grid = uint32_t(chunks == 0 ? 1 : (chunks < cap ? chunks : cap));
+            k<<<grid, kBlock, smem, s>>>(a, keys, out, n, wc);
+            return check_launch(C ? "contains kernel" : "find kernel");
+        } else {
+            return fail(B2CO_EINVAL, "bulk windows need 16-byte slots");
+        }
+    }
+
+    template <int B, bool C>
     static int find_shape(OaArgs const& a, uint32_t lanes, uint32_t items, void const* keys, uint8_t const* stencil,
                           void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
     {
+        bool const stageable = !stencil && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 && n >= kStageKeys && B > 1;
+        // bulk-window path: 16-byte slots only
+        if ((items & kShapeBulk) && stageable && S::bytes == 16) return find_bulk<B, C>(a, keys, out, n, wc, s);
+        items &= ~kShapeBulk;
         // staged path: no stencil, 16-byte aligned key stream, at least one stage of keys
-        bool const staged = !stencil && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 && n >= kStageKeys && B > 1 &&
-                            lanes >= 2;
+        bool const staged = stageable && lanes >= 2;
         if (staged) {
             bool const seg = (items & kShapeSegmented) != 0;
             items &= ~kShapeSegmented;

@@ -839,6 +839,157 @@ __global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys,
 }
 
 // ----------------------------------------------------------------------------
+// Bulk-window lookups (16-byte slots): every lane fetches its key's whole first
+// bucket window (B x 16 bytes, 16-byte aligned) with ONE bulk copy (TMA,
+// untiled) into shared memory.  Copies are tracked by the SM's bulk-copy
+// engine instead of the load/store unit, so a block keeps a whole stage of
+// 1024 windows in flight.  The 32 lanes of a warp arrive on one mbarrier per
+// batch; a lane resolves its own window from shared memory, and the rare key
+// that needs further windows continues with direct loads.  Keys are staged
+// by the same double-buffered bulk copies as k_find_staged.
+// ----------------------------------------------------------------------------
+
+constexpr int kBulkBatches = kStageKeys / 256;  // batches of 32 windows per warp per stage
+
+template <class S, int B>
+__host__ __device__ constexpr uint32_t bulk_window_smem()
+{
+    return 8u * kBulkBatches * 32u * uint32_t(B) * 16u;  // 8 warps x batches x 32 lanes x window
+}
+
+template <class S, int B, bool CONTAINS>
+__global__ void __launch_bounds__(256) k_find_bulk(OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
+{
+    static_assert(S::bytes == 16, "bulk windows need 16-byte slots (16-byte aligned windows)");
+    using Raw = typename S::Raw;
+    using Key = typename Io<S>::Key;
+    constexpr uint32_t WIN = uint32_t(B) * 16u;
+    __shared__ alignas(128) Key sk[2][kStageKeys];
+    __shared__ alignas(8) uint64_t kbar[2];
+    __shared__ alignas(8) uint64_t wbar[8][kBulkBatches];
+    __shared__ alignas(8) uint64_t never;
+    extern __shared__ __align__(128) unsigned char wins[];  // [warp][batch][lane][WIN]
+
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t const chunks = n / kStageKeys;
+    constexpr uint32_t kChunkBytes = kStageKeys * sizeof(Key);
+
+    if (threadIdx.x == 0) {
+        mbar_init(&kbar[0], 1);
+        mbar_init(&kbar[1], 1);
+        mbar_init(&never, 1);
+        for (int w = 0; w < 8; ++w)
+            for (int j = 0; j < kBulkBatches; ++j) mbar_init(&wbar[w][j], 32);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && blockIdx.x < chunks) {
+        mbar_arrive_expect_tx(&kbar[0], kChunkBytes);
+        bulk_g2s(sk[0], static_cast<Key const*>(keys) + uint64_t(blockIdx.x) * kStageKeys, kChunkBytes, &kbar[0]);
+    }
+    uint32_t it = 0;
+    bool failed = false, issued = false;
+    for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x, ++it) {
+        uint32_t const b = it & 1;
+        uint32_t const cn = c + gridDim.x;
+        issued = false;
+        if (threadIdx.x == 0 && cn < chunks) {
+            fence_proxy_async();
+            mbar_arrive_expect_tx(&kbar[b ^ 1], kChunkBytes);
+            bulk_g2s(sk[b ^ 1], static_cast<Key const*>(keys) + uint64_t(cn) * kStageKeys, kChunkBytes, &kbar[b ^ 1]);
+        }
+        bool ok = wc.probe_timeout ? mbar_wait_bounded(&never, 0, wc.ns)
+                                   : mbar_wait_bounded(&kbar[b], (it >> 1) & 1, wc.ns);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        issued = true;
+        Key const* ks = sk[b];
+        uint32_t const base = c * kStageKeys;
+        // issue every window copy of this warp's share of the stage
+        uint64_t key[kBulkBatches];
+        uint32_t init[kBulkBatches];
+        unsigned char* my_win = wins + (size_t(warp) * kBulkBatches * 32 + lane) * WIN;
+        fence_proxy_async();  // the previous stage's reads of the windows precede the new copies
+#pragma unroll
+        for (int j = 0; j < kBulkBatches; ++j) {
+            uint32_t const pos = (warp * kBulkBatches + j) * 32 + lane;
+            key[j] = ks[pos];
+            init[j] = probe_init<S::key_bytes, B>(a.probe, key[j]);
+            mbar_arrive_expect_tx(&wbar[warp][j], WIN);
+            bulk_g2s(my_win + size_t(j) * 32 * WIN, slots + init[j], WIN, &wbar[warp][j]);
+        }
+        // resolve batch by batch as the windows land
+#pragma unroll
+        for (int j = 0; j < kBulkBatches; ++j) {
+            ok = mbar_wait_bounded(&wbar[warp][j], it & 1, wc.ns);
+            uint32_t const pos = (warp * kBulkBatches + j) * 32 + lane;
+            uint64_t payload = empty_payload<S>(a);
+            bool hit = false;
+            if (ok) {
+                Raw const* w = reinterpret_cast<Raw const*>(my_win + size_t(j) * 32 * WIN);
+                int stop = -1;
+#pragma unroll
+                for (int s = B - 1; s >= 0; --s) {
+                    uint64_t k = S::key(w[s]);
+                    if (k == a.empty_key || k == key[j]) stop = s;
+                }
+                if (stop >= 0) {
+                    hit = S::key(w[stop]) != a.empty_key;
+                    if (hit) payload = S::value(w[stop]);
+                } else {
+                    hit = find_rest<S, B>(a, key[j], init[j], payload);
+                }
+            } else {
+                failed = true;
+            }
+            if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[base + pos] = hit;
+            else Io<S>::store_payload(out, base + pos, hit ? payload : empty_payload<S>(a));
+        }
+        if (__syncthreads_or(failed)) {
+            failed = true;
+            break;
+        }
+    }
+    if (failed) {
+        atomicExch(wc.status, kStatusTimeout);
+        // let this lane's and this block's copies land before the block exits (bounded again)
+        if (issued) {
+#pragma unroll
+            for (int j = 0; j < kBulkBatches; ++j) mbar_wait_bounded(&wbar[warp][j], it & 1, 1000000000ull);
+        }
+        if (threadIdx.x == 0) {
+            mbar_wait_bounded(&kbar[it & 1], (it >> 1) & 1, 1000000000ull);
+            if (blockIdx.x + (it + 1) * gridDim.x < chunks)
+                mbar_wait_bounded(&kbar[(it + 1) & 1], ((it + 1) >> 1) & 1, 1000000000ull);
+        }
+        return;
+    }
+    // ragged tail: block 0, one lane per key, direct loads
+    if (blockIdx.x == 0) {
+        for (uint32_t i = chunks * kStageKeys + threadIdx.x; i < n; i += blockDim.x) {
+            uint64_t const key = Io<S>::load_key(keys, i);
+            uint32_t const init0 = probe_init<S::key_bytes, B>(a.probe, key);
+            Raw w[B];
+            load_window<S, B>(slots, init0, w);
+            int j = scan_window<S, B>(w, key, a.empty_key);
+            uint64_t payload = empty_payload<S>(a);
+            bool hit;
+            if (j >= 0) {
+                hit = S::key(w[j]) != a.empty_key;
+                if (hit) payload = S::value(w[j]);
+            } else {
+                hit = find_rest<S, B>(a, key, init0, payload);
+            }
+            if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = hit;
+            else Io<S>::store_payload(out, i, hit ? payload : empty_payload<S>(a));
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
 // Erase (open_addressing_ref_impl.h:340-379) and Count (kernels.h:427-467)
 // ----------------------------------------------------------------------------
 

@@ -13,13 +13,14 @@ from helpers import dev, unique_keys
 pytestmark = pytest.mark.gpu
 
 
-def test_bounded_wait_reports_timeout_and_context_survives():
+@pytest.mark.parametrize("shape", [(8, 4, False, False), (1, 1, False, True)], ids=["staged", "bulk"])
+def test_bounded_wait_reports_timeout_and_context_survives(shape):
     import b2co
     import torch
     rng = np.random.default_rng(17)
     t = b2co.StaticMap(100000, -1, -1, key_dtype=torch.int64, value_dtype=torch.int64, probing=b2co.PROBE_DOUBLE,
                        hash_kind=b2co.HASH_XXH32)
-    t.set_find_shape(8, 4)  # the staged kernel
+    t.set_find_shape(*shape)  # the staged / bulk-window kernels wait on their own bulk copies
     keys = unique_keys(rng, 50000, 8)
     t.Insert(b2co.pack_pairs(dev(keys), dev(keys)))
     q = dev(keys[:8192])
