@@ -75,8 +75,8 @@ void default_shape(b2co_oa_table* t)
         t->find_lanes = 1;  // a one-slot window needs no cooperation
         t->find_items = 4;
     } else {
-        t->find_lanes = 8;  // one slot per lane, staged keys, 4 windows per tile in flight
-        t->find_items = 4;
+        t->find_lanes = 2;  // staged keys, two lanes per bucket window, two windows in flight per pair
+        t->find_items = 2;
     }
 }
 
