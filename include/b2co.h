@@ -131,6 +131,20 @@ int b2co_oa_insert_and_find(b2co_oa_table* table, const void* pairs, void* out_f
                             uint64_t n, int mode, b2co_stream stream);
 int b2co_oa_insert_and_find_async(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
                                   uint64_t n, int mode, b2co_stream stream);
+/* First-wins InsertAndFind that allocates nothing, for callers that cannot
+ * let a library allocate device memory (an application that owns all device
+ * memory through its own arena under a fixed budget, or a latency-critical
+ * path that must not pay for a device allocation).  No counterpart in the
+ * reference.  Same results as b2co_oa_insert_and_find(..., B2CO_IAF_FIRST_WINS)
+ * and synchronous like it, but the scratch (4 bytes per item, 4 + 1/8 bytes
+ * per table slot) comes from a fixed 32 MiB device array inside the library,
+ * which every GPU that loads the library holds until the process exits.
+ * Batches needing more scratch fail with B2CO_ERANGE.  The first call on a
+ * device looks up the array's address there; make that call before any stream
+ * capture begins.  All calls share the array, so calls that overlap on the GPU
+ * race: serialize them. */
+int b2co_oa_insert_and_find_noalloc(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
+                                    uint64_t n, b2co_stream stream);
 /* Erase (returns the count of keys not erased).
  * reference: static_map.h:292 Erase, :307 EraseAsync, open_addressing_impl.h:236-276, open_addressing_ref_impl.h:340-379. */
 int b2co_oa_erase(b2co_oa_table* table, const void* keys, uint64_t n, b2co_stream stream, uint64_t* failed);

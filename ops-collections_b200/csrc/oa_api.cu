@@ -131,6 +131,18 @@ int ensure_first_wins_scratch(b2co_oa_table* t, uint64_t n)
 
 }  // namespace
 
+// First-wins InsertAndFind on scratch the caller provides: pos[n],
+// newbits[ceil(capacity/32)] (cleared here) and owner[capacity].
+int b2co_oa_iaf_first_wins_on(b2co_oa_table* t, void const* pairs, void* out_found, uint8_t* out_inserted, uint64_t n,
+                              uint32_t* pos, uint32_t* newbits, uint32_t* owner, cudaStream_t s)
+{
+    if (int st = check_table(t)) return st;
+    if (int st = check_batch(n)) return st;
+    B2CO_CUDA(cudaMemsetAsync(newbits, 0, ((t->capacity + 31) / 32) * 4, s));
+    return t->ops->iaf_first(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), pos, newbits,
+                             owner, s);
+}
+
 // Table creation with the clear optional: DynamicMap prepares its next submap
 // uncleared and clears it on a side stream (the reference's DeferredClear
 // constructor, include/static_map.h:611).
