@@ -495,6 +495,70 @@ def extra_measurements(t, keys, q50, out, stream, args):
     q8 = make_queries(k8, N_QUERIES, 0.5, "torch")
     ms = timed(lambda: t.FindAsync(q8, out))
     res["find_lf08_hit50_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
+    del q8
+    res.update(bloom_hll_measurements(stream))
+    return res
+
+
+def bloom_hll_measurements(stream):
+    """The BloomFilter / HyperLogLog workload: a 2^30-bit filter (2^22 blocks of 256 bits)
+    with 2^28 uniform uint64 adds and 2^28 queries (half absent); an int64 HyperLogLog of
+    64 KiB (p = 16) with 2^30 adds drawn from 10^7 distinct keys, and a merge of 16
+    sub-sketches.  Size-independent checks: no false negatives, merge == one-shot."""
+    import torch
+    import b2co
+    peak, _ = peaks()
+    res = {}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def time_once(fn):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    nb, n = 1 << 22, 1 << 28
+    f = b2co.BloomFilter(nb, key_dtype=torch.int64)
+    adds = mix64_torch(counters(3 << 40, n, "torch"))
+    absent = mix64_torch(counters(4 << 40, n // 2, "torch"))
+    g = torch.Generator(device="cuda").manual_seed(SEED + 7)
+    q = torch.cat([adds[torch.randint(0, n, (n // 2,), generator=g, device="cuda")], absent])
+    f.AddAsync(adds[: 1 << 20])  # warm-up launch
+    f.Clear()
+    ms = time_once(lambda: f.AddAsync(adds))
+    res["bloom_add_gkeys"] = round(n / ms / 1e6, 3)
+    res["bloom_add_hbm_frac"] = round(n * 72 / (ms / 1e3) / 1e9 / peak, 4)
+    out = torch.empty(q.numel(), dtype=torch.uint8, device="cuda")
+    f.ContainsAsync(q, out)
+    ms = time_once(lambda: f.ContainsAsync(q, out))
+    res["bloom_contains_gkeys"] = round(q.numel() / ms / 1e6, 3)
+    res["bloom_contains_hbm_frac"] = round(q.numel() * 41 / (ms / 1e3) / 1e9 / peak, 4)
+    res["bloom_no_false_negatives"] = bool(out[: n // 2].all().item())
+    res["bloom_false_positive_rate"] = round(float(out[n // 2:].float().mean().item()), 6)
+    del adds, absent, q, out, f
+
+    distinct = mix64_torch(counters(5 << 40, 10_000_000, "torch"))
+    keys = distinct[torch.randint(0, distinct.numel(), (1 << 30,), generator=g, device="cuda")]
+    h = b2co.HyperLogLog(16)
+    h.AddAsync(keys[: 1 << 20])
+    h.Clear()
+    ms = time_once(lambda: h.AddAsync(keys))
+    res["hll_add_gkeys"] = round((1 << 30) / ms / 1e6, 3)
+    res["hll_add_hbm_frac"] = round((1 << 30) * 8 / (ms / 1e3) / 1e9 / peak, 4)
+    est = h.Estimate()
+    res["hll_estimate"] = est
+    res["hll_estimate_rel_err_vs_1e7"] = round(abs(est - 10_000_000) / 10_000_000, 5)
+    parts = [b2co.HyperLogLog(16) for _ in range(16)]
+    for i, p in enumerate(parts):
+        p.AddAsync(keys[i * (1 << 26):(i + 1) * (1 << 26)])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for p in parts[1:]:
+        parts[0].Merge(p)
+    res["hll_merge16_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+    res["hll_merge_equals_one_shot"] = bool(np.array_equal(parts[0].registers(), h.registers()))
     return res
 
 
@@ -544,7 +608,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b2co", choices=["b2co", "reference"])
     ap.add_argument("--shape", default="", help="Find kernel shape LANESxITEMS, e.g. 8x1")
