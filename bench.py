@@ -305,6 +305,9 @@ def run_gpu(args):
 
     q = make_queries(keys, N_QUERIES, 0.5, "torch")
     out = torch.empty(N_QUERIES, dtype=torch.int64, device="cuda")
+    if args.l2_fetch:
+        import b2co
+        b2co.set_l2_fetch_granularity(args.l2_fetch)
     if args.sweep:
         sweep = {}
         for shape in ["bulk", "2x2", "2x1", "4x1", "4x2", "8x4", "1x4"]:
@@ -497,6 +500,101 @@ def extra_measurements(t, keys, q50, out, stream, args):
     res["find_lf08_hit50_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
     del q8
     res.update(bloom_hll_measurements(stream))
+    res.update(batched_measurements(stream))
+    return res
+
+
+def mix32_torch(x):
+    """MurmurHash3 fmix32 over int64 tensors holding uint32 values: a bijection on 32 bits."""
+    m = 0xFFFFFFFF
+    x = x & m
+    x = x ^ (x >> 16)
+    x = (x * 0x85EBCA6B) & m
+    x = x ^ (x >> 13)
+    x = (x * 0xC2B2AE35) & m
+    return x ^ (x >> 16)
+
+
+def batched_measurements(stream):
+    """Batched tables: 4,096 StaticMap<int32,int32> (DoubleHashing<xxhash_32>, bucket 5)
+    at load factor 0.5 with log-normal key counts (median 32,768, sigma(log2) = 2.0,
+    clipped to [1,024; 4,194,304]); each table inserts its own keys, then finds 2x its
+    key count at 50% hits.  One persistent group launch (and its CUDA-graph replay,
+    lane count from the autotuner) against one plain launch per table."""
+    import torch
+    import b2co
+    rng = np.random.default_rng(SEED + 11)
+    count = 4096
+    sizes = np.clip(np.round(np.exp2(rng.normal(15.0, 2.0, size=count))), 1024, 4194304).astype(np.int64)
+    total = int(sizes.sum())
+    ins_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    q_off = 2 * ins_off
+    # keys of table t: fmix32 of a per-table counter range (distinct within the
+    # table, uniform), skipping the -1 sentinel; misses from the next range
+    t_of = torch.repeat_interleave(torch.arange(count, device="cuda"), torch.from_numpy(sizes).cuda())
+    j = torch.arange(total, device="cuda") - torch.from_numpy(ins_off[:-1]).cuda()[t_of]
+    salt = (t_of * 0x9E3779B1) & 0xFFFFFFFF
+    k32 = mix32_torch(j ^ salt)
+    k32 = torch.where(k32 == 0xFFFFFFFF, mix32_torch((j + (1 << 31)) ^ salt), k32)
+    keys = k32.to(torch.int32)  # two's-complement wrap of the uint32 value
+    vals = (k32 >> 1).to(torch.int32)  # never the -1 sentinel
+    pairs = b2co.pack_pairs(keys, vals)
+    del t_of, j, salt, k32, vals
+    g = torch.Generator(device="cuda").manual_seed(SEED + 12)
+    qt = torch.repeat_interleave(torch.arange(count, device="cuda"), 2 * torch.from_numpy(sizes).cuda())
+    qj = torch.arange(2 * total, device="cuda") - torch.from_numpy(q_off[:-1]).cuda()[qt]
+    n_t = torch.from_numpy(sizes).cuda()[qt]
+    base = torch.from_numpy(ins_off[:-1]).cuda()[qt]
+    hit = qj < n_t
+    rnd = torch.randint(0, 1 << 40, (2 * total,), generator=g, device="cuda")
+    hit_keys = keys[base + rnd % n_t]
+    qsalt = (qt * 0x9E3779B1) & 0xFFFFFFFF
+    miss = mix32_torch((qj + (1 << 30)) ^ qsalt).to(torch.int64).to(torch.int32)  # j >= 2^30 never used above
+    q = torch.where(hit, hit_keys, miss)
+    del qt, qj, n_t, base, rnd, hit_keys, qsalt, miss
+    d_ins_off = torch.from_numpy(ins_off).cuda()
+    d_q_off = torch.from_numpy(q_off).cuda()
+    out = torch.empty(2 * total, dtype=torch.int32, device="cuda")
+    ref = torch.empty(2 * total, dtype=torch.int32, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    grp = b2co.TableGroup(2 * sizes, -1, -1, key_dtype=torch.int32, value_dtype=torch.int32)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    failed = grp.Insert(pairs, d_ins_off, sync=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    res = {"batched_tables": count, "batched_total_keys": total, "batched_total_queries": 2 * total,
+           "batched_group_insert_gkeys": round(total / e0.elapsed_time(e1) / 1e6, 3)}
+    per = b2co.TableGroup(2 * sizes, -1, -1, key_dtype=torch.int32, value_dtype=torch.int32)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    per.InsertPerTable(pairs, ins_off.astype(np.uint64))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    res["batched_per_table_insert_gkeys"] = round(total / e0.elapsed_time(e1) / 1e6, 3)
+    lanes = grp.Autotune(q, d_q_off, ref)
+    res["batched_autotuned_lanes"] = lanes
+    ms = timed(lambda: grp.Find(q, d_q_off, out))
+    res["batched_group_find_gkeys"] = round(2 * total / ms / 1e6, 3)
+    ms = timed(lambda: grp.Find(q, d_q_off, out, graph=True))
+    res["batched_graph_find_gkeys"] = round(2 * total / ms / 1e6, 3)
+    res["batched_graph_equals_group"] = bool(torch.equal(out, ref))
+    out2 = torch.empty_like(out)
+    ms = timed(lambda: per.FindPerTable(q, q_off.astype(np.uint64), out2), reps=2)
+    res["batched_per_table_find_gkeys"] = round(2 * total / ms / 1e6, 3)
+    res["batched_per_table_equals_group"] = bool(torch.equal(out2, ref))
+    res["batched_hits_found"] = bool(((ref != -1) == hit).all().item())
     return res
 
 
@@ -620,6 +718,7 @@ def main():
     ap.add_argument("--capacity-log2", type=int, default=28, help="requested capacity 2^k (profiling: smaller)")
     ap.add_argument("--queries-log2", type=int, default=27, help="queries per step 2^k (profiling: smaller)")
     ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
+    ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("warmup must be >= 3")

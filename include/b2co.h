@@ -65,6 +65,14 @@ const char* b2co_version(void);
  * hook: the first wait of each block is made on a barrier that nothing ever
  * arrives on, so the timeout path runs without any fault. */
 int b2co_debug_set_wait(uint64_t limit_ns, int probe_timeout);
+/* Context-wide hint of the bytes the L2 fetches from DRAM per miss (32, 64 or
+ * 128; 0 = only read the current value into *applied).  Random bucket windows
+ * use a fraction of a 128-byte line, so a smaller granularity cuts the DRAM
+ * traffic of lookups.  It applies to the calling process's whole CUDA context
+ * on the current device (not to the GPU beyond the process), so it is the
+ * application's choice; the library never sets it on its own.  No reference
+ * counterpart. */
+int b2co_set_l2_fetch_granularity(uint32_t bytes, uint64_t* applied);
 
 /* ===================================================================== */
 /* Open-addressing tables: StaticMap<K,T> and StaticSet<K>                 */
@@ -187,6 +195,48 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
  * copy into shared memory; tables with 16-byte slots only (others ignore it). */
 #define B2CO_FIND_BULK 0x200u
 int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_lane);
+
+/* ===================================================================== */
+/* Table groups: many independent tables, one launch per operation          */
+/* ===================================================================== */
+/* The batched pattern (thousands of StaticMap/StaticSet tables of uneven
+ * sizes, e.g. per-partition group-by or join builds).  Each table keeps the
+ * single-table semantics of b2co_oa_*; the group packs them into one slab and
+ * serves an operation on all tables with one persistent launch.  Items of
+ * table t are [offsets[t], offsets[t+1]) of a concatenated input (count + 1
+ * offsets).  No reference counterpart: the reference runs one launch per
+ * container call. */
+typedef struct b2co_oa_group b2co_oa_group;
+
+int b2co_oa_group_create(const b2co_oa_desc* desc, const uint64_t* requested_capacities, uint32_t count,
+                         b2co_stream stream, b2co_oa_group** out);
+int b2co_oa_group_destroy(b2co_oa_group* group);
+int b2co_oa_group_table_capacity(const b2co_oa_group* group, uint32_t table, uint64_t* capacity);
+int b2co_oa_group_total_slots(const b2co_oa_group* group, uint64_t* slots);
+/* The slab: table t's slots start at the sum of the capacities of tables < t. */
+int b2co_oa_group_data(const b2co_oa_group* group, void** slab);
+int b2co_oa_group_clear(b2co_oa_group* group, b2co_stream stream);
+/* Insert into every table (device offsets); with `failed` non-NULL the call
+ * synchronizes and returns the total failed count. */
+int b2co_oa_group_insert(b2co_oa_group* group, const void* pairs, const uint64_t* d_offsets, uint64_t n,
+                         b2co_stream stream, uint64_t* failed);
+/* Find (contains = 0) or Contains (contains = 1) on every table, one launch. */
+int b2co_oa_group_find(b2co_oa_group* group, const void* keys, const uint64_t* d_offsets, void* out, uint64_t n,
+                       int contains, b2co_stream stream);
+/* The same launch replayed from a CUDA graph captured on first use. */
+int b2co_oa_group_find_graph(b2co_oa_group* group, const void* keys, const uint64_t* d_offsets, void* out,
+                             uint64_t n, int contains, b2co_stream stream);
+/* One plain launch per table (host offsets): the baseline the group launch replaces. */
+int b2co_oa_group_find_per_table(b2co_oa_group* group, const void* keys, const uint64_t* h_offsets, void* out,
+                                 int contains, b2co_stream stream);
+int b2co_oa_group_insert_per_table(b2co_oa_group* group, const void* pairs, const uint64_t* h_offsets,
+                                   b2co_stream stream);
+/* Lanes per key of the group Find (1, 2, 4 or 8). */
+int b2co_oa_group_set_find_shape(b2co_oa_group* group, uint32_t lanes);
+/* Autotuner: times every lane count on this batch, keeps the fastest, and
+ * leaves valid results in `out`. */
+int b2co_oa_group_autotune_find(b2co_oa_group* group, const void* keys, const uint64_t* d_offsets, void* out,
+                                uint64_t n, b2co_stream stream, uint32_t* chosen_lanes);
 
 /* ===================================================================== */
 /* BloomFilter<Key>, default policy (8 x uint32 words per block, xxh64)     */

@@ -149,6 +149,16 @@ def pack_pairs(keys, values):
     return out
 
 
+def set_l2_fetch_granularity(nbytes: int) -> int:
+    """Context-wide hint of how many bytes the L2 fetches from DRAM per miss
+    (32, 64 or 128).  Random bucket windows waste most of a 128-byte line; a
+    smaller granularity cuts DRAM traffic per lookup.  Applies to the whole
+    process's CUDA context, so it is the application's choice to make."""
+    v = C.c_uint64()
+    _call("b2co_set_l2_fetch_granularity", C.c_uint32(nbytes), C.byref(v))
+    return v.value
+
+
 def valid_capacity(requested: int, bucket_size: int = 5, probing: int = PROBE_DOUBLE) -> int:
     c = C.c_uint64()
     _call("b2co_oa_valid_capacity", C.c_uint64(requested), C.c_uint32(bucket_size), C.c_uint32(probing),
@@ -350,6 +360,85 @@ class StaticSet(_OaBase):
         import torch
         super().__init__(capacity, empty_key, 0, key_dtype or torch.int32, None, bucket_size, probing, hash_kind,
                          erased_key, stream)
+
+
+class TableGroup:
+    """Many independent StaticMap/StaticSet tables served by one launch per
+    operation (include/b2co.h, b2co_oa_group_*).  `capacities` are the
+    requested capacities per table; items of table t are the slice
+    [offsets[t], offsets[t+1]) of a concatenated input."""
+
+    def __init__(self, capacities, empty_key, empty_value, key_dtype=None, value_dtype=None, bucket_size=5,
+                 probing=PROBE_DOUBLE, hash_kind=HASH_XXH32, stream=None):
+        import torch
+        key_dtype = key_dtype or torch.int32
+        kb = _dtype_bytes(key_dtype)
+        vb = 0 if value_dtype is None else _dtype_bytes(value_dtype)
+        self.key_bytes, self.value_bytes = kb, vb
+        caps = np.ascontiguousarray(capacities, dtype=np.uint64)
+        d = OaDesc(kb, vb, bucket_size, probing, hash_kind, 0, _bits(empty_key, kb),
+                   _bits(empty_value, vb) if vb else 0, _bits(empty_key, kb))
+        h = C.c_void_p()
+        _call("b2co_oa_group_create", C.byref(d), C.c_void_p(caps.ctypes.data), C.c_uint32(len(caps)),
+              _stream(stream), C.byref(h))
+        self._h = h
+        self.count = len(caps)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_oa_group_destroy(h)
+            self._h = None
+
+    def table_capacity(self, t):
+        v = C.c_uint64()
+        _call("b2co_oa_group_table_capacity", self._h, C.c_uint32(t), C.byref(v))
+        return v.value
+
+    def total_slots(self):
+        v = C.c_uint64()
+        _call("b2co_oa_group_total_slots", self._h, C.byref(v))
+        return v.value
+
+    def Data(self) -> int:
+        p = C.c_void_p()
+        _call("b2co_oa_group_data", self._h, C.byref(p))
+        return p.value
+
+    def dump_slots(self) -> np.ndarray:
+        return _device_bytes(self.Data(), self.total_slots() * slot_bytes(self.key_bytes, self.value_bytes))
+
+    def Clear(self, stream=None):
+        _call("b2co_oa_group_clear", self._h, _stream(stream))
+
+    def Insert(self, pairs, d_offsets, stream=None, sync=True):
+        f = C.c_uint64()
+        _call("b2co_oa_group_insert", self._h, _ptr(pairs), _ptr(d_offsets), C.c_uint64(pairs.shape[0]),
+              _stream(stream), C.byref(f) if sync else None)
+        return f.value if sync else None
+
+    def Find(self, keys, d_offsets, out, contains=False, stream=None, graph=False):
+        name = "b2co_oa_group_find_graph" if graph else "b2co_oa_group_find"
+        _call(name, self._h, _ptr(keys), _ptr(d_offsets), _ptr(out), C.c_uint64(keys.shape[0]),
+              C.c_int(1 if contains else 0), _stream(stream))
+
+    def FindPerTable(self, keys, h_offsets: np.ndarray, out, contains=False, stream=None):
+        h = np.ascontiguousarray(h_offsets, dtype=np.uint64)
+        _call("b2co_oa_group_find_per_table", self._h, _ptr(keys), C.c_void_p(h.ctypes.data), _ptr(out),
+              C.c_int(1 if contains else 0), _stream(stream))
+
+    def InsertPerTable(self, pairs, h_offsets: np.ndarray, stream=None):
+        h = np.ascontiguousarray(h_offsets, dtype=np.uint64)
+        _call("b2co_oa_group_insert_per_table", self._h, _ptr(pairs), C.c_void_p(h.ctypes.data), _stream(stream))
+
+    def set_find_shape(self, lanes):
+        _call("b2co_oa_group_set_find_shape", self._h, C.c_uint32(lanes))
+
+    def Autotune(self, keys, d_offsets, out, stream=None) -> int:
+        v = C.c_uint32()
+        _call("b2co_oa_group_autotune_find", self._h, _ptr(keys), _ptr(d_offsets), _ptr(out),
+              C.c_uint64(keys.shape[0]), _stream(stream), C.byref(v))
+        return v.value
 
 
 class DynamicMap:

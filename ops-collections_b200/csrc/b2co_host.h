@@ -73,4 +73,16 @@ struct OaOps {
 
 extern OaOps const kOpsSet4, kOpsSet8, kOpsMap44, kOpsMap48, kOpsMap84, kOpsMap88;
 
+struct GroupArgs;
+
+// Launchers of the persistent group kernels for one slot layout.
+struct GroupOps {
+    int (*find)(GroupArgs const& g, uint32_t b, uint32_t lanes, bool contains, void const* keys, void* out,
+                uint64_t n, cudaStream_t s);
+    int (*insert)(GroupArgs const& g, uint32_t b, void const* pairs, uint64_t n, unsigned long long* failed,
+                  cudaStream_t s);
+};
+
+extern GroupOps const kGroupSet4, kGroupSet8, kGroupMap44, kGroupMap48, kGroupMap84, kGroupMap88;
+
 }  // namespace b2co

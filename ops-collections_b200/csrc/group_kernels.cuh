@@ -1,0 +1,138 @@
+// group_kernels.cuh -- persistent kernels over a group of independent tables
+// (thousands of StaticMaps of uneven sizes in one slab, the batched pattern of
+// per-partition group-by / join builds).
+//
+// One launch covers every table: the items of all tables are concatenated
+// (table t owns items [offsets[t], offsets[t+1])) and each warp takes one
+// contiguous span of the concatenation, so work is balanced by items, not by
+// tables.  A lane finds its table once by binary search and then only walks
+// forward; the table's probe parameters stay in registers while it does not
+// change.  Per key the algorithms are exactly the single-table ones.
+#pragma once
+
+#include "oa_kernels.cuh"
+
+namespace b2co {
+
+struct GroupTable {
+    uint64_t slot_offset;  // first slot of the table in the slab
+    ProbeParams probe;
+};
+
+struct GroupArgs {
+    void* slots;
+    GroupTable const* tables;
+    uint64_t const* offsets;  // count + 1 item offsets (device)
+    uint32_t count;
+    uint64_t empty_key;
+    uint64_t empty_value;
+};
+
+__device__ __forceinline__ uint32_t group_table_of(uint64_t const* offsets, uint32_t count, uint64_t i)
+{
+    uint32_t lo = 0, hi = count;  // offsets[lo] <= i < offsets[hi]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(offsets + mid) <= i) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <class S>
+__device__ __forceinline__ OaArgs group_table_args(GroupArgs const& g, uint32_t t)
+{
+    OaArgs a;
+    GroupTable const& d = g.tables[t];
+    a.slots = static_cast<typename S::Raw*>(g.slots) + d.slot_offset;
+    a.probe = d.probe;
+    a.empty_key = g.empty_key;
+    a.empty_value = g.empty_value;
+    a.erased_key = g.empty_key;
+    return a;
+}
+
+// Span of the concatenation owned by this warp: multiples of `step` items.
+__device__ __forceinline__ void warp_span(uint64_t n, uint32_t step, uint64_t& begin, uint64_t& end)
+{
+    uint64_t const warps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+    uint64_t const warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    uint64_t span = (n + warps - 1) / warps;
+    span = (span + step - 1) / step * step;
+    begin = warp * span;
+    end = begin + span < n ? begin + span : n;
+}
+
+template <class S, int B, int G, bool CONTAINS>
+__global__ void __launch_bounds__(256) k_group_find(GroupArgs g, void const* keys, void* out, uint64_t n)
+{
+    using Raw = typename S::Raw;
+    constexpr int ROUNDS = (B + G - 1) / G;
+    constexpr uint32_t TILES = 32 / G;
+    uint32_t const lane = threadIdx.x & 31, r = lane % G, tile_lane0 = lane & ~uint32_t(G - 1), tile = lane / G;
+    uint64_t begin, end;
+    warp_span(n, TILES, begin, end);
+    if (begin >= end) return;  // warp-uniform
+    uint32_t t = group_table_of(g.offsets, g.count, begin + tile < end ? begin + tile : begin);
+    OaArgs a = group_table_args<S>(g, t);
+    uint64_t next_off = __ldg(g.offsets + t + 1);
+    for (uint64_t i0 = begin; i0 < end; i0 += TILES) {
+        uint64_t const i = i0 + tile;
+        bool const live = i < end;
+        if (live && i >= next_off) {
+            do {
+                ++t;
+                next_off = __ldg(g.offsets + t + 1);
+            } while (i >= next_off);
+            a = group_table_args<S>(g, t);
+        }
+        uint64_t const key = live ? uint64_t(__ldg(reinterpret_cast<typename Io<S>::Key const*>(keys) + i)) : 0;
+        uint32_t const init = live ? probe_init<S::key_bytes, B>(a.probe, key) : 0;
+        Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+        Raw w[ROUNDS];
+        if (live) {
+#pragma unroll
+            for (int k = 0; k < ROUNDS; ++k)
+                if (int(r) + k * G < B) w[k] = ld_ro(slots + init + r + k * G);
+        }
+        TileResult res{0, false, !live};
+        tile_resolve<S, B, G, ROUNDS>(a, w, key, r, tile_lane0, !live, res);
+        if (__any_sync(0xffffffffu, !res.done)) res = tile_continue<S, B, G, ROUNDS>(a, slots, key, init, r, tile_lane0, res);
+        if (r == 0 && live) {
+            if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = res.hit;
+            else reinterpret_cast<typename Io<S>::Payload*>(out)[i] =
+                typename Io<S>::Payload(res.hit ? res.payload : empty_payload<S>(a));
+        }
+    }
+}
+
+template <class S, int B>
+__global__ void __launch_bounds__(256) k_group_insert(GroupArgs g, void const* pairs, uint64_t n,
+                                                      unsigned long long* failed_counter)
+{
+    uint64_t begin, end;
+    warp_span(n, 32, begin, end);
+    uint32_t failed = 0;
+    if (begin < end) {
+        uint32_t const lane = threadIdx.x & 31;
+        uint32_t t = group_table_of(g.offsets, g.count, begin + lane < end ? begin + lane : begin);
+        OaArgs a = group_table_args<S>(g, t);
+        uint64_t next_off = __ldg(g.offsets + t + 1);
+        for (uint64_t i0 = begin; i0 < end; i0 += 32) {
+            uint64_t const i = i0 + lane;
+            if (i >= end) continue;
+            if (i >= next_off) {
+                do {
+                    ++t;
+                    next_off = __ldg(g.offsets + t + 1);
+                } while (i >= next_off);
+                a = group_table_args<S>(g, t);
+            }
+            typename S::Raw p = ld_ro(reinterpret_cast<typename S::Raw const*>(pairs) + i);
+            failed += insert_one<S, B, false>(a, S::key(p), S::value(p)) != kSuccess;
+        }
+    }
+    if (failed_counter) warp_add_counter(failed_counter, failed);
+}
+
+}  // namespace b2co

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "b2co_host.h"
+#include "group_kernels.cuh"
 #include "oa_kernels.cuh"
 
 namespace b2co {
@@ -202,9 +203,50 @@ struct OaImpl {
     static constexpr OaOps ops{&clear, &insert, &assign_if, &iaf_race, &iaf_first, &find, &erase, &count};
 };
 
+template <class S>
+struct GroupImpl {
+    static constexpr uint32_t kBlock = 256;
+
+    template <int B, bool C>
+    static int find_b(GroupArgs const& g, uint32_t lanes, void const* keys, void* out, uint64_t n, cudaStream_t s)
+    {
+        void (*k)(GroupArgs, void const*, void*, uint64_t) = nullptr;
+        if (lanes <= 1) k = k_group_find<S, B, 1, C>;
+        else if (lanes == 2) k = k_group_find<S, B, 2, C>;
+        else if (lanes == 4) k = k_group_find<S, B, 4, C>;
+        else k = k_group_find<S, B, 8, C>;
+        // persistent: every resident block, spans balanced by items
+        k<<<grid_for((void const*)k, kBlock, n, 1), kBlock, 0, s>>>(g, keys, out, n);
+        return OaImpl<S>::check_launch(C ? "group contains kernel" : "group find kernel");
+    }
+
+    static int find(GroupArgs const& g, uint32_t b, uint32_t lanes, bool contains, void const* keys, void* out,
+                    uint64_t n, cudaStream_t s)
+    {
+        return OaImpl<S>::with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            return contains ? find_b<B, true>(g, lanes, keys, out, n, s) : find_b<B, false>(g, lanes, keys, out, n, s);
+        });
+    }
+
+    static int insert(GroupArgs const& g, uint32_t b, void const* pairs, uint64_t n, unsigned long long* failed,
+                      cudaStream_t s)
+    {
+        return OaImpl<S>::with_b(b, [&](auto bc) {
+            constexpr int B = decltype(bc)::value;
+            auto k = k_group_insert<S, B>;
+            k<<<grid_for((void const*)k, kBlock, n, 1), kBlock, 0, s>>>(g, pairs, n, failed);
+            return OaImpl<S>::check_launch("group insert kernel");
+        });
+    }
+
+    static constexpr GroupOps ops{&find, &insert};
+};
+
 }  // namespace b2co
 
-#define B2CO_DEFINE_OA_OPS(NAME, KB, VB) \
-    namespace b2co {                     \
-    OaOps const NAME = OaImpl<SlotT<KB, VB>>::ops; \
+#define B2CO_DEFINE_OA_OPS(NAME, GNAME, KB, VB)            \
+    namespace b2co {                                       \
+    OaOps const NAME = OaImpl<SlotT<KB, VB>>::ops;         \
+    GroupOps const GNAME = GroupImpl<SlotT<KB, VB>>::ops;  \
     }

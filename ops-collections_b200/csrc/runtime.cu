@@ -163,6 +163,19 @@ const char* b2co_status_string(int s)
 
 const char* b2co_version(void) { return "b2co 0.1 (sm_100a)"; }
 
+int b2co_set_l2_fetch_granularity(uint32_t bytes, uint64_t* applied)
+{
+    if (bytes != 0 && bytes != 32 && bytes != 64 && bytes != 128)
+        return b2co::fail(B2CO_EINVAL, "L2 fetch granularity must be 32, 64 or 128 bytes");
+    if (bytes) B2CO_CUDA(cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, bytes));
+    if (applied) {
+        size_t v = 0;
+        B2CO_CUDA(cudaDeviceGetLimit(&v, cudaLimitMaxL2FetchGranularity));
+        *applied = v;
+    }
+    return B2CO_OK;
+}
+
 int b2co_debug_set_wait(uint64_t limit_ns, int probe_timeout)
 {
     b2co::g_wait_ns.store(limit_ns ? limit_ns : 1000000000ull);
