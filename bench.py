@@ -215,10 +215,11 @@ def parse_shape(s: str):
     """'LxK', 'LxKs' or 'bulk': L lanes per key, K keys in flight per lane group,
     s = segmented windows, bulk = one bulk copy per bucket window."""
     if s == "bulk":
-        return 1, 1, False, True
+        return 1, 1, False, True, False
+    warp = s.endswith("w")
     seg = s.endswith("s")
-    lanes, items = (int(x) for x in s.rstrip("s").split("x"))
-    return lanes, items, seg, False
+    lanes, items = (int(x) for x in s.rstrip("sw").split("x"))
+    return lanes, items, seg, False, warp
 
 
 def peaks():
@@ -310,7 +311,7 @@ def run_gpu(args):
         b2co.set_l2_fetch_granularity(args.l2_fetch)
     if args.sweep:
         sweep = {}
-        for shape in ["bulk", "2x2", "2x1", "4x1", "4x2", "8x4", "1x4"]:
+        for shape in ["2x2", "2x2w", "2x1w", "4x1w", "4x2w", "4x4w", "8x4w", "4x2", "2x2s"]:
             t.set_find_shape(*parse_shape(shape))
             for _ in range(3):
                 t.FindAsync(q, out)

@@ -194,6 +194,8 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
 /* OR-ed into keys_per_lane: fetch every first bucket window with one bulk (TMA)
  * copy into shared memory; tables with 16-byte slots only (others ignore it). */
 #define B2CO_FIND_BULK 0x200u
+/* OR-ed into keys_per_lane: every warp stages its own key chunks (no block barrier). */
+#define B2CO_FIND_WARP_STAGED 0x400u
 int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_lane);
 
 /* ===================================================================== */

@@ -32,6 +32,7 @@ IAF_RACE, IAF_FIRST_WINS = 0, 1
 INSERT_EXACT_DEDUP, INSERT_APPEND_UNIQUE = 0, 1
 FIND_SEGMENTED = 0x100
 FIND_BULK = 0x200
+FIND_WARP_STAGED = 0x400
 
 
 class B2coError(Exception):
@@ -305,8 +306,10 @@ class _OaBase:
         _call("b2co_oa_find_host", self._h, C.c_void_p(host_keys.ctypes.data), C.c_void_p(host_out.ctypes.data),
               C.c_uint64(n), _stream(stream))
 
-    def set_find_shape(self, lanes_per_key: int, keys_per_lane: int, segmented: bool = False, bulk: bool = False):
-        flags = (FIND_SEGMENTED if segmented else 0) | (FIND_BULK if bulk else 0)
+    def set_find_shape(self, lanes_per_key: int, keys_per_lane: int, segmented: bool = False, bulk: bool = False,
+                       warp_staged: bool = False):
+        flags = (FIND_SEGMENTED if segmented else 0) | (FIND_BULK if bulk else 0) | \
+            (FIND_WARP_STAGED if warp_staged else 0)
         _call("b2co_oa_set_find_shape", self._h, C.c_uint32(lanes_per_key), C.c_uint32(keys_per_lane | flags))
 
     @staticmethod

@@ -51,6 +51,8 @@ constexpr uint32_t kShapeSegmented = 0x100;
 // Lookup shape flag: fetch every first bucket window with one bulk (TMA) copy
 // into shared memory (16-byte slots; B2CO_FIND_BULK in the C ABI).
 constexpr uint32_t kShapeBulk = 0x200;
+// Lookup shape flag: every warp stages its own keys (B2CO_FIND_WARP_STAGED).
+constexpr uint32_t kShapeWarpStaged = 0x400;
 
 // Launchers for one slot layout; B (bucket size) is dispatched at run time.
 struct OaOps {

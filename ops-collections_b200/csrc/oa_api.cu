@@ -469,7 +469,7 @@ int b2co_oa_set_find_shape(b2co_oa_table* t, uint32_t lanes, uint32_t items)
         return B2CO_OK;
     }
     if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) return fail(B2CO_EINVAL, "lanes must be 1, 2, 4 or 8");
-    uint32_t const k = items & ~(kShapeSegmented | kShapeBulk);
+    uint32_t const k = items & ~(kShapeSegmented | kShapeBulk | kShapeWarpStaged);
     if (k != 1 && k != 2 && k != 4) return fail(B2CO_EINVAL, "keys per lane must be 1, 2 or 4");
     t->find_lanes = lanes;
     t->find_items = items;

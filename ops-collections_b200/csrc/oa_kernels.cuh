@@ -592,26 +592,47 @@ __device__ __forceinline__ void tile_resolve(OaArgs const& a, typename S::Raw co
     }
 }
 
-// Segment-wise scan of one window: slots [lo, hi) of the window starting at
-// slot `idx`, loaded one slot per lane (at most G slots per call).  DRAM serves
-// random reads in 64-byte bursts, and an 80-byte bucket always spans two, so
-// the first call covers only the slots up to the next 64-byte boundary and the
-// second runs only for tiles whose first segment neither held the key nor an
-// empty slot.
-template <class S, int G>
-__device__ __forceinline__ void resolve_segment(OaArgs const& a, typename S::Raw w, bool own, uint64_t key, uint32_t r,
-                                                uint32_t lane0, bool skip, TileResult& res)
+// Line-split scan of a first window (the SEG variant).  DRAM reads for random
+// lookups arrive as whole 128-byte L2 lines, and an 80-byte bucket straddles two
+// lines half of the time; the split variant reads the part in the first line,
+// and the part in the second line only for windows the first part did not
+// settle.
+//
+// Slots [lo, hi) of a window, lane r holding slots lo + r + t*G (t < ROUNDS):
+// loads them and finds the first one that ends the scan, as tile_resolve does
+// for a whole window.
+template <class S, int B, int G, int ROUNDS>
+__device__ __forceinline__ void load_range(typename S::Raw const* slots, uint32_t idx, int lo, int hi, uint32_t r,
+                                           bool skip, typename S::Raw (&w)[ROUNDS])
+{
+#pragma unroll
+    for (int t = 0; t < ROUNDS; ++t)
+        if (!skip && lo + int(r) + t * G < hi) w[t] = ld_ro(slots + idx + lo + r + t * G);
+}
+
+template <class S, int B, int G, int ROUNDS>
+__device__ __forceinline__ void resolve_range(OaArgs const& a, typename S::Raw const (&w)[ROUNDS], int lo, int hi,
+                                              uint64_t key, uint32_t r, uint32_t lane0, bool skip, TileResult& res)
 {
     constexpr uint32_t MASK = (1u << G) - 1u;
-    own = own && !skip;
-    uint64_t const k = own ? S::key(w) : 0;
-    bool const is_stop = own && (k == a.empty_key || k == key);
-    bool const is_hit = is_stop && k != a.empty_key;
-    uint32_t const stop_bits = (__ballot_sync(0xffffffffu, is_stop) >> lane0) & MASK;
-    uint32_t const hit_bits = (__ballot_sync(0xffffffffu, is_hit) >> lane0) & MASK;
+    uint32_t stop_bits = 0, hit_bits = 0;
+#pragma unroll
+    for (int t = 0; t < ROUNDS; ++t) {
+        bool const own = !skip && lo + int(r) + t * G < hi;
+        uint64_t const k = own ? S::key(w[t]) : 0;
+        bool const is_stop = own && (k == a.empty_key || k == key);
+        bool const is_hit = is_stop && k != a.empty_key;
+        stop_bits |= ((__ballot_sync(0xffffffffu, is_stop) >> lane0) & MASK) << (t * G);
+        hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> lane0) & MASK) << (t * G);
+    }
     int const s = stop_bits ? __ffs(stop_bits) - 1 : -1;
-    uint64_t const mine = (s >= 0 && int(r) == s) ? S::value(w) : 0;
-    uint64_t const got = __shfl_sync(0xffffffffu, (unsigned long long)mine, lane0 + (s >= 0 ? s : 0));
+    uint64_t mine = 0;
+    if (s >= 0 && int(r) == s % G) {
+#pragma unroll
+        for (int t = 0; t < ROUNDS; ++t)
+            if (t == s / G) mine = S::value(w[t]);
+    }
+    uint64_t const got = __shfl_sync(0xffffffffu, (unsigned long long)mine, lane0 + (s >= 0 ? s % G : 0));
     if (!skip && s >= 0) {
         res.done = true;
         res.hit = (hit_bits >> s) & 1u;
@@ -619,26 +640,13 @@ __device__ __forceinline__ void resolve_segment(OaArgs const& a, typename S::Raw
     }
 }
 
-// End of the segment that starts at window slot `lo`: the next 64-byte
-// boundary, the window's end, or G slots further, whichever comes first.
-template <class S, int B, int G>
-__device__ __forceinline__ int segment_end(uint32_t idx, int lo)
+// Slots of the window starting at `idx` before the next 128-byte L2 line boundary.
+template <class S, int B>
+__device__ __forceinline__ int slots_to_line_end(uint32_t idx)
 {
-    constexpr int per = 64 / S::bytes;
-    int hi = lo + per - int((idx + lo) % per);
-    if (hi > lo + G) hi = lo + G;
-    return hi < B ? hi : B;
-}
-
-template <class S, int B, int G>
-__device__ __forceinline__ void tile_segment(OaArgs const& a, typename S::Raw const* slots, uint32_t idx, int lo,
-                                             int hi, uint64_t key, uint32_t r, uint32_t lane0, bool skip,
-                                             TileResult& res)
-{
-    bool const own = !skip && lo + int(r) < hi;
-    typename S::Raw w{};
-    if (own) w = ld_ro(slots + idx + lo + r);
-    resolve_segment<S, G>(a, w, own, key, r, lane0, skip, res);
+    constexpr int per = 128 / S::bytes;
+    int const n1 = per - int(idx % per);
+    return n1 < B ? n1 : B;
 }
 
 // Further windows of keys whose first window neither held the key nor an
@@ -731,46 +739,29 @@ __global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys,
 #pragma unroll
             for (int q = 0; q < Q; ++q) idx[q] = init[q] = __shfl_sync(0xffffffffu, my_init, tile_lane0 + q);
             if constexpr (SEG) {
-                // first segment of every key's first window in flight together
-                Raw w1[Q];
+                // phase 1: every key's first window up to its L2 line end, all in flight together
+                Raw w[Q][ROUNDS];
                 int hi1[Q];
-#pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    hi1[q] = segment_end<S, B, G>(idx[q], 0);
-                    w1[q] = Raw{};
-                    if (int(r) < hi1[q]) w1[q] = ld_ro(slots + idx[q] + r);
-                }
                 TileResult res[Q];
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
+                    hi1[q] = slots_to_line_end<S, B>(idx[q]);
+                    load_range<S, B, G, ROUNDS>(slots, idx[q], 0, hi1[q], r, false, w[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < Q; ++q) {
                     res[q] = TileResult{0, false, false};
-                    resolve_segment<S, G>(a, w1[q], int(r) < hi1[q], key[q], r, tile_lane0, false, res[q]);
+                    resolve_range<S, B, G, ROUNDS>(a, w[q], 0, hi1[q], key[q], r, tile_lane0, false, res[q]);
                 }
-                // second segment only where the first did not end the scan, again all in flight
-                Raw w2[Q];
-                int lo2[Q], hi2[Q];
+                // phase 2: the part in the next line, only for windows the first part did not settle
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    load_range<S, B, G, ROUNDS>(slots, idx[q], hi1[q], B, r, res[q].done, w[q]);
 #pragma unroll
                 for (int q = 0; q < Q; ++q) {
-                    lo2[q] = hi1[q];
-                    bool const act = !res[q].done && lo2[q] < B;
-                    hi2[q] = act ? segment_end<S, B, G>(idx[q], lo2[q]) : lo2[q];
-                    w2[q] = Raw{};
-                    if (act && lo2[q] + int(r) < hi2[q]) w2[q] = ld_ro(slots + idx[q] + lo2[q] + r);
-                }
-#pragma unroll
-                for (int q = 0; q < Q; ++q) {
-                    if (__any_sync(0xffffffffu, !res[q].done && lo2[q] < B)) {
-                        bool const act = !res[q].done && lo2[q] < B;
-                        resolve_segment<S, G>(a, w2[q], act && lo2[q] + int(r) < hi2[q], key[q], r, tile_lane0, !act,
-                                              res[q]);
-                        int lo = hi2[q];
-                        while (__any_sync(0xffffffffu, !res[q].done && lo < B)) {  // windows wider than two segments
-                            bool const more = !res[q].done && lo < B;
-                            int const hi = more ? segment_end<S, B, G>(idx[q], lo) : lo;
-                            tile_segment<S, B, G>(a, slots, idx[q], lo, hi, key[q], r, tile_lane0, !more, res[q]);
-                            lo = hi;
-                        }
-                    }
+                    if (__any_sync(0xffffffffu, !res[q].done && hi1[q] < B))
+                        resolve_range<S, B, G, ROUNDS>(a, w[q], hi1[q], B, key[q], r, tile_lane0,
+                                                       res[q].done || hi1[q] >= B, res[q]);
                     if (__any_sync(0xffffffffu, !res[q].done))  // rare: further windows
                         res[q] = tile_continue<S, B, G, ROUNDS>(a, slots, key[q], init[q], r, tile_lane0, res[q]);
                     if (r == 0) {
@@ -828,6 +819,127 @@ __global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys,
             }
             TileResult res{0, false, !live};
             tile_resolve<S, B, G, ROUNDS>(a, w, key, r, tile_lane0, !live, res);
+            if (__any_sync(0xffffffffu, !res.done))
+                res = tile_continue<S, B, G, ROUNDS>(a, slots, key, init0, r, tile_lane0, res);
+            if (r == 0 && live) {
+                if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = res.hit;
+                else Io<S>::store_payload(out, i, res.hit ? res.payload : empty_payload<S>(a));
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Warp-staged lookups: like k_find_staged, but every warp stages its own
+// 256-key chunks (double-buffered bulk copies, one mbarrier per buffer), so
+// warps never wait for each other -- no block barrier, no straggler stalls
+// when one warp's keys need further windows.
+// ----------------------------------------------------------------------------
+
+constexpr uint32_t kWarpStageKeys = 256;
+
+template <class S, int B, int G, int Q, bool CONTAINS>
+__global__ void __launch_bounds__(256) k_find_wstaged(OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
+{
+    static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");
+    using Raw = typename S::Raw;
+    using Key = typename Io<S>::Key;
+    constexpr int ROUNDS = (B + G - 1) / G;
+    constexpr uint32_t TILES = 32 / G;   // tiles per warp
+    constexpr uint32_t PASS = TILES * Q;  // keys per warp pass
+    static_assert(kWarpStageKeys % PASS == 0, "stage must hold whole passes");
+    constexpr uint32_t kChunkBytes = kWarpStageKeys * sizeof(Key);
+    __shared__ alignas(128) Key sk[8][2][kWarpStageKeys];
+    __shared__ alignas(8) uint64_t bar[8][2];
+    __shared__ alignas(8) uint64_t never[8];
+
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t const r = lane % G, tile_lane0 = lane & ~uint32_t(G - 1), tile = lane / G;
+    uint32_t const gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t const nwarps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t const chunks = n / kWarpStageKeys;
+    Key const* kin = static_cast<Key const*>(keys);
+
+    if (lane == 0) {
+        mbar_init(&bar[warp][0], 1);
+        mbar_init(&bar[warp][1], 1);
+        mbar_init(&never[warp], 1);
+        fence_mbar_init();
+        if (gwarp < chunks) {
+            mbar_arrive_expect_tx(&bar[warp][0], kChunkBytes);
+            bulk_g2s(sk[warp][0], kin + uint64_t(gwarp) * kWarpStageKeys, kChunkBytes, &bar[warp][0]);
+        }
+    }
+    __syncwarp();
+    uint32_t it = 0;
+    bool failed = false;
+    for (uint32_t c = gwarp; c < chunks; c += nwarps, ++it) {
+        uint32_t const b = it & 1;
+        uint32_t const cn = c + nwarps;
+        if (lane == 0 && cn < chunks) {
+            fence_proxy_async();  // the warp's reads of this buffer (previous chunk) precede the copy
+            mbar_arrive_expect_tx(&bar[warp][b ^ 1], kChunkBytes);
+            bulk_g2s(sk[warp][b ^ 1], kin + uint64_t(cn) * kWarpStageKeys, kChunkBytes, &bar[warp][b ^ 1]);
+        }
+        bool const ok = wc.probe_timeout ? mbar_wait_bounded(&never[warp], 0, wc.ns)
+                                         : mbar_wait_bounded(&bar[warp][b], (it >> 1) & 1, wc.ns);
+        if (__any_sync(0xffffffffu, !ok)) {
+            failed = true;
+            break;
+        }
+        Key const* ks = sk[warp][b];
+        uint32_t const base = c * kWarpStageKeys;
+        for (uint32_t p = 0; p < kWarpStageKeys; p += PASS) {
+            uint64_t key[Q];
+            uint32_t idx[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) key[q] = ks[p + q * TILES + tile];
+            uint32_t my_init = 0;
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                if (int(r) == q) my_init = probe_init<S::key_bytes, B>(a.probe, key[q]);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) idx[q] = __shfl_sync(0xffffffffu, my_init, tile_lane0 + q);
+            Raw w[Q][ROUNDS];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) load_range<S, B, G, ROUNDS>(slots, idx[q], 0, B, r, false, w[q]);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                TileResult res{0, false, false};
+                resolve_range<S, B, G, ROUNDS>(a, w[q], 0, B, key[q], r, tile_lane0, false, res);
+                if (__any_sync(0xffffffffu, !res.done))  // rare: further windows
+                    res = tile_continue<S, B, G, ROUNDS>(a, slots, key[q], idx[q], r, tile_lane0, res);
+                if (r == 0) {
+                    uint32_t const i = base + p + q * TILES + tile;
+                    if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = res.hit;
+                    else Io<S>::store_payload(out, i, res.hit ? res.payload : empty_payload<S>(a));
+                }
+            }
+        }
+        __syncwarp();  // every lane is done with this buffer before it is refilled
+    }
+    if (failed) {
+        if (lane == 0) {
+            atomicExch(wc.status, kStatusTimeout);
+            // let this warp's copies still in flight land before the block can exit (bounded again)
+            uint32_t const c = gwarp + it * nwarps;
+            mbar_wait_bounded(&bar[warp][it & 1], (it >> 1) & 1, 1000000000ull);
+            if (c + nwarps < chunks) mbar_wait_bounded(&bar[warp][(it + 1) & 1], ((it + 1) >> 1) & 1, 1000000000ull);
+        }
+        return;
+    }
+    // the ragged tail (< one warp stage) goes to one warp, keys read directly
+    if (chunks * kWarpStageKeys < n && gwarp == chunks % nwarps) {
+        for (uint32_t i0 = chunks * kWarpStageKeys; i0 < n; i0 += TILES) {
+            uint32_t const i = i0 + tile;
+            bool const live = i < n;
+            uint64_t const key = live ? Io<S>::load_key(keys, i) : 0;
+            uint32_t const init0 = live ? probe_init<S::key_bytes, B>(a.probe, key) : 0;
+            Raw w[ROUNDS];
+            load_range<S, B, G, ROUNDS>(slots, init0, 0, B, r, !live, w);
+            TileResult res{0, false, !live};
+            resolve_range<S, B, G, ROUNDS>(a, w, 0, B, key, r, tile_lane0, !live, res);
             if (__any_sync(0xffffffffu, !res.done))
                 res = tile_continue<S, B, G, ROUNDS>(a, slots, key, init0, r, tile_lane0, res);
             if (r == 0 && live) {

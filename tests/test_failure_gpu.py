@@ -13,7 +13,8 @@ from helpers import dev, unique_keys
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("shape", [(8, 4, False, False), (1, 1, False, True)], ids=["staged", "bulk"])
+@pytest.mark.parametrize("shape", [(8, 4, False, False, False), (1, 1, False, True, False),
+                                   (2, 2, False, False, True)], ids=["staged", "bulk", "warp_staged"])
 def test_bounded_wait_reports_timeout_and_context_survives(shape):
     import b2co
     import torch

@@ -269,10 +269,11 @@ def test_find_shapes_agree():
         o = oracle_table(t, kb, vb, b, oracle.PROBE_DOUBLE, oracle.HASH_XXH32)
         o.insert(keys, vals)
         ref = (o.find(q)[0], o.contains(q)[0])
-        shapes = [(l, i, False, False) for l in (1, 2, 4, 8) for i in (1, 2, 4)] + \
-                 [(l, i, True, False) for l in (2, 4, 8) for i in (1, 2, 4)] + [(1, 1, False, True)]
-        for lanes, items, seg, bulk in shapes:
-            t.set_find_shape(lanes, items, seg, bulk)
+        shapes = [(l, i, False, False, False) for l in (1, 2, 4, 8) for i in (1, 2, 4)] + \
+                 [(l, i, True, False, False) for l in (2, 4, 8) for i in (1, 2, 4)] + \
+                 [(l, i, False, False, True) for l in (2, 4, 8) for i in (1, 2, 4)] + [(1, 1, False, True, False)]
+        for lanes, items, seg, bulk, warp in shapes:
+            t.set_find_shape(lanes, items, seg, bulk, warp)
             out = out_buf(len(q), kb, vb)
             t.Find(qd, out)
             c = torch.empty(len(q), dtype=torch.uint8, device="cuda")
