@@ -502,6 +502,7 @@ def extra_measurements(t, keys, q50, out, stream, args):
     del q8
     res.update(bloom_hll_measurements(stream))
     res.update(batched_measurements(stream))
+    res.update(served_measurements(stream))
     return res
 
 
@@ -665,6 +666,135 @@ def bloom_hll_measurements(stream):
 # reference arm: the reference algorithm's CPU restatement on the host cores
 # ---------------------------------------------------------------------------
 
+SERVED_RATES = (1000, 2000, 5000, 10000, 20000, 50000, 200000)  # the last one is past saturation
+SERVED_STREAM, SERVED_MISS, SERVED_NEW, SERVED_VALUES = 3 << 40, 4 << 40, 5 << 40, 6 << 40
+
+
+def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, inflight=8):
+    """Served tables: 8 resident StaticMap<int64,int64> (DoubleHashing<xxhash_32>,
+    bucket 5) of 10M..200M pairs (geometric spacing) at load factor 0.6, 15 GB in
+    all, behind one b2co Server (HBM budget 150 GB, `inflight` launch streams,
+    at most 4 Mi keys per coalesced launch).  Requests arrive as a Poisson
+    stream at each swept rate for `seconds`; sizes are log-normal (median
+    31,623 keys, sigma 1.15) clipped to [1e3, 1e6]; 90% Find / 10%
+    InsertOrAssign, tables uniform, keys at a 70% hit rate (misses from a
+    disjoint stream; IOA non-hits are new keys).  Payloads come from a pool of
+    `pool` pinned host requests reused round-robin; the schedule is submitted
+    in chunks of 32 (submit_many), chunk c after chunk c - pool/32 completed
+    (its buffers are reused).  Latency = done - scheduled arrival (queueing
+    included); keys/s = all keys / (last done - first arrival)."""
+    import torch
+    import b2co
+    rng = np.random.default_rng(SEED + 5)
+    sizes = np.geomspace(10e6, 200e6, 8).astype(np.int64)
+    tables = []
+    t_build = time.time()
+    for j, n in enumerate(sizes):
+        m = b2co.StaticMap(int(n / 0.6), -1, -1, key_dtype=torch.int64, value_dtype=torch.int64, bucket_size=5,
+                           probing=b2co.PROBE_DOUBLE, hash_kind=b2co.HASH_XXH32)
+        k = mix64_torch(counters(SERVED_STREAM + (j << 32), int(n), "torch"))
+        v = mix64_torch(counters(SERVED_VALUES + (j << 32), int(n), "torch"))
+        p = b2co.pack_pairs(k, v)
+        del k, v
+        assert m.Insert(p) == 0
+        del p
+        tables.append(m)
+    torch.cuda.synchronize()
+    table_gb = sum(m.Capacity() * 16 for m in tables) / 1e9
+    log(f"[served] 8 tables, {int(sizes.sum())} pairs, {table_gb:.1f} GB, built in {time.time() - t_build:.1f} s")
+
+    # request pool: one pinned arena for inputs, one for outputs
+    ops = np.where(rng.random(pool) < 0.1, b2co.OP_INSERT_OR_ASSIGN, b2co.OP_FIND)
+    tabs = rng.integers(0, 8, size=pool)
+    ns = np.clip(np.exp(rng.normal(math.log(31623), 1.15, size=pool)), 1e3, 1e6).astype(np.int64)
+    in_words = np.where(ops == b2co.OP_FIND, ns, 2 * ns)
+    in_arena = b2co.pinned((int(in_words.sum()),), np.int64)
+    out_arena = b2co.pinned((int(ns.sum()),), np.int64)
+    pool_desc = np.zeros(pool, dtype=b2co.REQUEST_DESC)
+    io, oo, new_ctr = 0, 0, 0
+    for i in range(pool):
+        n, j = int(ns[i]), int(tabs[i])
+        hit = rng.random(n) < 0.7
+        other = SERVED_MISS if ops[i] == b2co.OP_FIND else SERVED_NEW
+        idx = np.where(hit, SERVED_STREAM + (j << 32) + rng.integers(0, sizes[j], size=n),
+                       other + new_ctr + np.arange(n))
+        new_ctr += n
+        keys = mix64_np(idx)
+        inp = in_arena[io:io + in_words[i]]
+        io += int(in_words[i])
+        if ops[i] == b2co.OP_FIND:
+            inp[:] = keys
+            out_ptr = out_arena[oo:oo + n].ctypes.data
+            oo += n
+        else:
+            pr = inp.reshape(n, 2)
+            pr[:, 0] = keys
+            pr[:, 1] = mix64_np(SERVED_VALUES + (7 << 32) + np.arange(n) + i * (1 << 20))
+            out_ptr = 0
+        pool_desc[i] = (tables[j]._h.value, int(ops[i]), 0, inp.ctypes.data, out_ptr, n, 0)
+
+    srv = b2co.Server(max_inflight=inflight, hbm_budget_bytes=150 * 10**9, max_batch_keys=1 << 22)
+    for m in tables:
+        srv.register(m)
+    chunk = 32  # requests per submit_many / wait_many call
+    assert pool % chunk == 0
+    ring = pool // chunk
+
+    def run_rate(rate, count):
+        count = -(-count // chunk) * chunk
+        t0 = b2co.Server.now_ns() + 5_000_000
+        arrivals = (t0 + np.cumsum(rng.exponential(1e9 / rate, size=count))).astype(np.uint64)
+        ids, infos, late = [], [], 0
+        s0 = srv.stats()
+        for c in range(count // chunk):
+            if c >= ring:
+                infos.append(srv.wait_many(ids[c - ring]))
+            d = pool_desc[(c % ring) * chunk:(c % ring + 1) * chunk].copy()
+            d["arrival_ns"] = arrivals[c * chunk:(c + 1) * chunk]
+            late += int(b2co.Server.now_ns() > int(d["arrival_ns"][0]))
+            ids.append(srv.submit_many(d))
+        infos += [srv.wait_many(x) for x in ids[max(0, len(ids) - ring):]]
+        s1 = srv.stats()
+        inf = np.concatenate(infos)
+        assert (inf["status"] == 0).all()
+        lat = (inf["done_ns"] - inf["arrival_ns"]).astype(np.float64) / 1e6
+        queued = (inf["admit_ns"] - inf["arrival_ns"]).astype(np.float64) / 1e6
+        service = lat - queued
+        is_find = inf["op"] == b2co.OP_FIND
+        keys = int(inf["n"].sum())
+        span = float(inf["done_ns"].max() - inf["arrival_ns"].min()) / 1e9
+        launches = s1["launches"] - s0["launches"]
+        return {"offered_req_s": rate, "requests": count, "achieved_req_s": round(count / span, 1),
+                "keys_per_s": round(keys / span, 1), "gkeys_s": round(keys / span / 1e9, 4),
+                "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                "find_p99_ms": round(float(np.percentile(lat[is_find], 99)), 3),
+                "p99_queue_ms": round(float(np.percentile(queued, 99)), 3),
+                "p99_service_ms": round(float(np.percentile(service, 99)), 3),
+                "max_ms": round(float(lat.max()), 3), "chunks_submitted_late": late,
+                "launches": launches, "requests_per_launch": round(count / max(1, launches), 2),
+                "host_us_per_launch": round((s1["total_launch_host_ns"] - s0["total_launch_host_ns"])
+                                            / max(1, launches) / 1e3, 1),
+                "copies": s1["copies"] - s0["copies"]}
+
+    run_rate(rates[0], 128)  # warm-up: first launches of every table
+    out = []
+    for rate in rates:
+        r = run_rate(rate, max(200, int(rate * seconds)))
+        log(f"[served] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s, "
+            f"{r['requests_per_launch']} req/launch, {r['host_us_per_launch']} us host/launch")
+        out.append(r)
+    st = srv.stats()
+    srv.close()
+    del tables
+    torch.cuda.empty_cache()
+    return {"served": {"tables": [int(x) for x in sizes], "table_gb": round(table_gb, 2), "load_factor": 0.6,
+                       "inflight_streams": inflight, "max_batch_keys": 1 << 22, "hbm_budget_gb": 150,
+                       "request_pool": pool, "mean_request_keys": round(float(np.mean(ns)), 1),
+                       "seconds_per_rate": seconds, "host_buffers": "pinned",
+                       "staging_grows": st["staging_grows"], "max_loop_gap_us": round(st["max_loop_gap_ns"] / 1e3, 1),
+                       "sweep": out}}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -720,12 +850,19 @@ def main():
     ap.add_argument("--queries-log2", type=int, default=27, help="queries per step 2^k (profiling: smaller)")
     ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
+    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll"],
+                    help="run one secondary measurement alone and print its JSON (not the headline line)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("warmup must be >= 3")
     global REQ_CAPACITY, N_QUERIES
     REQ_CAPACITY, N_QUERIES = 1 << args.capacity_log2, 1 << args.queries_log2
-    if args.impl == "reference":
+    if args.only:
+        import torch
+        fn = {"served": served_measurements, "batched": batched_measurements,
+              "bloom_hll": bloom_hll_measurements}[args.only]
+        print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

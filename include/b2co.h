@@ -241,6 +241,80 @@ int b2co_oa_group_autotune_find(b2co_oa_group* group, const void* keys, const ui
                                 uint64_t n, b2co_stream stream, uint32_t* chosen_lanes);
 
 /* ===================================================================== */
+/* Request server over resident tables                                      */
+/* ===================================================================== */
+/* The serving pattern: requests of uneven sizes against resident tables,
+ * admitted as launch slots and an HBM budget free up, with the arrived
+ * Find/Contains requests on one table coalesced into one launch (never past a
+ * write on that table: each request sees exactly the writes that arrived
+ * before it), and work of many requests overlapping on the device.  A request
+ * carries its arrival time (b2co_server_now_ns() clock; 0 = now), so a whole
+ * arrival schedule can be submitted ahead of time; requests must be submitted
+ * in arrival order.  Host buffers should be pinned.  No reference
+ * counterpart. */
+typedef enum { B2CO_OP_FIND = 0, B2CO_OP_CONTAINS = 1, B2CO_OP_INSERT = 2, B2CO_OP_INSERT_OR_ASSIGN = 3 } b2co_op;
+typedef struct {
+    uint64_t id;
+    int32_t op;
+    int32_t status;       /* b2co_status of the request */
+    uint64_t n;
+    uint64_t arrival_ns;  /* b2co_server_now_ns() clock */
+    uint64_t admit_ns;
+    uint64_t done_ns;     /* when the dispatcher saw the launch complete */
+    uint64_t failed;      /* Insert / InsertOrAssign counts */
+    uint64_t assigned;
+} b2co_request_info;
+typedef struct b2co_server b2co_server;
+
+uint64_t b2co_server_now_ns(void);
+/* max_inflight launch slots (streams); staging plus registered tables never
+ * exceed hbm_budget_bytes; coalesced lookups hold at most max_batch_keys keys
+ * (0 = 16 Mi).  Every slot's staging buffer is allocated here, sized for a full
+ * coalesced lookup batch (at most a quarter of the budget in all). */
+int b2co_server_create(uint32_t max_inflight, uint64_t hbm_budget_bytes, uint64_t max_batch_keys, b2co_server** out);
+/* Counts a resident table's bytes against the budget. */
+int b2co_server_register_table(b2co_server* server, b2co_oa_table* table);
+/* host_in: keys (Find/Contains) or pairs (Insert/InsertOrAssign); host_out:
+ * payloads (Find) or 1-byte flags (Contains), unused otherwise. */
+int b2co_server_submit(b2co_server* server, b2co_oa_table* table, int op, const void* host_in, void* host_out,
+                       uint64_t n, uint64_t arrival_ns, uint64_t* request_id);
+/* Blocks until the request completes; fills *info and releases the id. */
+int b2co_server_wait(b2co_server* server, uint64_t request_id, b2co_request_info* info);
+/* One request of a batched submission (the arguments of b2co_server_submit). */
+typedef struct {
+    b2co_oa_table* table;
+    int32_t op;
+    int32_t reserved;  /* 0 */
+    const void* host_in;
+    void* host_out;
+    uint64_t n;
+    uint64_t arrival_ns;
+} b2co_request_desc;
+/* Submits `count` requests under one lock, all or none (the first invalid one
+ * fails the call); ids[i] is requests[i]'s id. */
+int b2co_server_submit_many(b2co_server* server, uint64_t count, const b2co_request_desc* requests, uint64_t* ids);
+/* Waits for every id; infos may be NULL.  Returns B2CO_OK, or the status of
+ * the first request that failed (all ids are released either way). */
+int b2co_server_wait_many(b2co_server* server, uint64_t count, const uint64_t* ids, b2co_request_info* infos);
+int b2co_server_stats(b2co_server* server, uint64_t* launches, uint64_t* requests_launched, uint64_t* bytes_in_use);
+/* Dispatcher observability, cumulative since creation. */
+typedef struct {
+    uint64_t launches;
+    uint64_t requests_launched;
+    uint64_t bytes_in_use;          /* registered tables + staging buffers */
+    uint64_t staging_bytes;         /* staging buffers held by the launch slots */
+    uint64_t staging_grows;         /* staging (re)allocations */
+    uint64_t max_launch_host_ns;    /* longest host time issuing one launch (copies, kernel, event) */
+    uint64_t max_reserve_host_ns;   /* longest host time growing a staging buffer */
+    uint64_t max_loop_gap_ns;       /* longest interval between two dispatcher polls */
+    uint64_t total_launch_host_ns;  /* host time issuing all launches */
+    uint64_t copies;                /* host<->device copies issued */
+} b2co_server_stats_ex;
+int b2co_server_get_stats_ex(b2co_server* server, b2co_server_stats_ex* stats);
+/* Finishes every submitted request, then stops the dispatcher. */
+int b2co_server_destroy(b2co_server* server);
+
+/* ===================================================================== */
 /* BloomFilter<Key>, default policy (8 x uint32 words per block, xxh64)     */
 /* ===================================================================== */
 

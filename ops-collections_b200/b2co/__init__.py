@@ -87,6 +87,7 @@ def lib():
         L.b2co_last_error.restype = C.c_char_p
         L.b2co_status_string.restype = C.c_char_p
         L.b2co_version.restype = C.c_char_p
+        L.b2co_server_now_ns.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -442,6 +443,120 @@ class TableGroup:
         _call("b2co_oa_group_autotune_find", self._h, _ptr(keys), _ptr(d_offsets), _ptr(out),
               C.c_uint64(keys.shape[0]), _stream(stream), C.byref(v))
         return v.value
+
+
+OP_FIND, OP_CONTAINS, OP_INSERT, OP_INSERT_OR_ASSIGN = 0, 1, 2, 3
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("op", C.c_int32), ("status", C.c_int32), ("n", C.c_uint64),
+                ("arrival_ns", C.c_uint64), ("admit_ns", C.c_uint64), ("done_ns", C.c_uint64),
+                ("failed", C.c_uint64), ("assigned", C.c_uint64)]
+
+
+# numpy layouts of b2co_request_desc / b2co_request_info (batched submit / wait)
+REQUEST_DESC = np.dtype([("table", "u8"), ("op", "i4"), ("reserved", "i4"), ("host_in", "u8"), ("host_out", "u8"),
+                         ("n", "u8"), ("arrival_ns", "u8")])
+REQUEST_INFO = np.dtype([("id", "u8"), ("op", "i4"), ("status", "i4"), ("n", "u8"), ("arrival_ns", "u8"),
+                         ("admit_ns", "u8"), ("done_ns", "u8"), ("failed", "u8"), ("assigned", "u8")])
+
+
+class Server:
+    """Request server over resident tables (include/b2co.h, b2co_server_*).
+    Host buffers passed to submit() must stay alive (and should be pinned)
+    until the request completes."""
+
+    _STATS_EX = ("launches", "requests_launched", "bytes_in_use", "staging_bytes", "staging_grows",
+                 "max_launch_host_ns", "max_reserve_host_ns", "max_loop_gap_ns", "total_launch_host_ns", "copies")
+
+    def __init__(self, max_inflight=8, hbm_budget_bytes=150 << 30, max_batch_keys=0):
+        L = lib()
+        L.b2co_server_submit.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_uint64,
+                                         C.c_uint64, C.POINTER(C.c_uint64)]
+        L.b2co_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(RequestInfo)]
+        L.b2co_server_submit_many.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.b2co_server_wait_many.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+        h = C.c_void_p()
+        _call("b2co_server_create", C.c_uint32(max_inflight), C.c_uint64(hbm_budget_bytes),
+              C.c_uint64(max_batch_keys), C.byref(h))
+        self._h = h
+        self._keep = {}
+        self._rid = C.c_uint64()
+
+    @staticmethod
+    def now_ns() -> int:
+        """The server clock (steady, ns) that arrival times are given in."""
+        return lib().b2co_server_now_ns()
+
+    def register(self, table):
+        _call("b2co_server_register_table", self._h, table._h)
+
+    def submit(self, table, op, host_in: np.ndarray, host_out=None, arrival_ns: int = 0) -> int:
+        """Queues a request; the arrays are kept alive until wait() returns."""
+        rid = self.submit_ptr(table._h.value, op, host_in.ctypes.data,
+                              None if host_out is None else host_out.ctypes.data, host_in.shape[0], arrival_ns)
+        self._keep[rid] = (host_in, host_out)
+        return rid
+
+    def submit_ptr(self, table_handle: int, op: int, in_ptr: int, out_ptr, n: int, arrival_ns: int = 0) -> int:
+        """submit() on raw host addresses; the caller keeps the buffers alive."""
+        st = _lib.b2co_server_submit(self._h, table_handle, op, in_ptr, out_ptr, n, arrival_ns, self._rid)
+        if st != OK:
+            _check(st)
+        return self._rid.value
+
+    def wait(self, rid: int) -> RequestInfo:
+        info = RequestInfo()
+        st = _lib.b2co_server_wait(self._h, rid, info)
+        self._keep.pop(rid, None)
+        if st != OK:
+            _check(st)
+        return info
+
+    def submit_many(self, descs: np.ndarray) -> np.ndarray:
+        """Submits a REQUEST_DESC array (table = a table's handle value, host
+        addresses as integers) in one call; the caller keeps the buffers alive.
+        Returns the ids."""
+        descs = np.ascontiguousarray(descs, dtype=REQUEST_DESC)
+        ids = np.empty(len(descs), dtype=np.uint64)
+        st = _lib.b2co_server_submit_many(self._h, len(descs), descs.ctypes.data, ids.ctypes.data)
+        if st != OK:
+            _check(st)
+        return ids
+
+    def wait_many(self, ids, check: bool = True) -> np.ndarray:
+        """Waits for every id; a REQUEST_INFO array.  With check, raises the
+        first failed request's error after all have been waited for."""
+        ids = np.ascontiguousarray(ids, dtype=np.uint64)
+        infos = np.zeros(len(ids), dtype=REQUEST_INFO)
+        st = _lib.b2co_server_wait_many(self._h, len(ids), ids.ctypes.data, infos.ctypes.data)
+        for rid in ids.tolist():
+            self._keep.pop(rid, None)
+        if st != OK and check:
+            _check(st)
+        return infos
+
+    def stats(self):
+        """b2co_server_get_stats_ex as a dict."""
+        v = (C.c_uint64 * len(self._STATS_EX))()
+        _call("b2co_server_get_stats_ex", self._h, v)
+        return dict(zip(self._STATS_EX, list(v)))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value and _lib is not None:
+            _lib.b2co_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+def pinned(shape, dtype):
+    """A numpy array in pinned (page-locked) host memory."""
+    import torch
+    tdt = {np.dtype(np.int64): torch.int64, np.dtype(np.int32): torch.int32, np.dtype(np.uint8): torch.uint8}[
+        np.dtype(dtype)]
+    return torch.empty(shape, dtype=tdt).pin_memory().numpy()
 
 
 class DynamicMap:

@@ -143,6 +143,32 @@ int b2co_oa_iaf_first_wins_on(b2co_oa_table* t, void const* pairs, void* out_fou
                              owner, s);
 }
 
+// Insert / InsertOrAssign with caller-owned device counters [failed, assigned]
+// (zeroed by the caller), so concurrent launches on one table keep separate
+// counts; nothing is synchronized.
+int b2co_oa_launch_insert(b2co_oa_table* t, void const* pairs, uint64_t n, bool assign,
+                          unsigned long long* d_counters, cudaStream_t s)
+{
+    if (int st = check_table(t)) return st;
+    if (n == 0 || !pairs) return B2CO_OK;
+    if (int st = check_batch(n)) return st;
+    return t->ops->insert(t->args, t->desc.bucket_size, pairs, nullptr, uint32_t(n), assign, d_counters, s);
+}
+
+// Device bytes a table holds (slots and counters).
+uint64_t b2co_oa_table_bytes(b2co_oa_table const* t)
+{
+    return t ? t->capacity * slot_bytes(t->desc.key_bytes, t->desc.value_bytes) + 3 * sizeof(unsigned long long) : 0;
+}
+
+// Key / payload / pair sizes of a table.
+void b2co_oa_table_sizes(b2co_oa_table const* t, uint32_t* key_bytes, uint32_t* payload_bytes, uint32_t* pair_bytes)
+{
+    *key_bytes = t->desc.key_bytes;
+    *payload_bytes = t->desc.value_bytes ? t->desc.value_bytes : t->desc.key_bytes;
+    *pair_bytes = slot_bytes(t->desc.key_bytes, t->desc.value_bytes);
+}
+
 // Table creation with the clear optional: DynamicMap prepares its next submap
 // uncleared and clears it on a side stream (the reference's DeferredClear
 // constructor, include/static_map.h:611).
