@@ -1,5 +1,5 @@
 // group.cu -- C ABI of table groups: many independent StaticMap/StaticSet
-// tables of uneven sizes served by one persistent launch (SURVEY's batched
+// tables of uneven sizes served by one persistent launch (the batched
 // pattern: per-partition group-by / join builds).
 //
 // Every table keeps the single-table semantics (capacity from the prime rule,
