@@ -431,10 +431,25 @@ def host_side_checks(t, q, out, args):
             o.find_parallel(qa[done:done + chunk], threads)
             done += chunk
         el = time.perf_counter() - t0
+        st_n = 1 << 21  # single thread: the sequential oracle Find on a 2 Mi-query slice
+        t1 = time.perf_counter()
+        o.find(qa[:st_n])
+        st_el = time.perf_counter() - t1
         cpu = {"value": round(done / el / 1e9, 5), "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"{done} of the 2^27 timed queries (50% hits) over a host copy of the same LF0.5 table, "
-                         f"oracle Find on {threads} OpenMP threads, {el:.1f} s"}
+                         f"oracle Find on {threads} OpenMP threads, {el:.1f} s",
+               "single_thread_value": round(st_n / st_el / 1e9, 5), "cpu_model": cpu_model()}
     return windows_mean, cpu, parity
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 def extra_measurements(t, keys, q50, out, stream, args):
@@ -600,11 +615,12 @@ def batched_measurements(stream):
     return res
 
 
-def bloom_hll_measurements(stream):
+def bloom_hll_measurements(stream, bloom=True, hll_log2=30):
     """The BloomFilter / HyperLogLog workload: a 2^30-bit filter (2^22 blocks of 256 bits)
     with 2^28 uniform uint64 adds and 2^28 queries (half absent); an int64 HyperLogLog of
-    64 KiB (p = 16) with 2^30 adds drawn from 10^7 distinct keys, and a merge of 16
-    sub-sketches.  Size-independent checks: no false negatives, merge == one-shot."""
+    64 KiB (p = 16) with 2^hll_log2 (default 2^30) adds drawn from 10^7 distinct keys, and
+    a merge of 16 sub-sketches.  Size-independent checks: no false negatives, merge ==
+    one-shot.  `bloom=False` runs the HyperLogLog part alone (profiling)."""
     import torch
     import b2co
     peak, _ = peaks()
@@ -619,11 +635,43 @@ def bloom_hll_measurements(stream):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
+    g = torch.Generator(device="cuda").manual_seed(SEED + 7)
+    if bloom:
+        res.update(bloom_part(f_time=time_once, g=g, peak=peak))
+    n_hll = 1 << hll_log2
+    distinct = mix64_torch(counters(5 << 40, 10_000_000, "torch"))
+    keys = distinct[torch.randint(0, distinct.numel(), (n_hll,), generator=g, device="cuda")]
+    h = b2co.HyperLogLog(16)
+    h.AddAsync(keys[: 1 << 20])
+    h.Clear()
+    ms = time_once(lambda: h.AddAsync(keys))
+    res["hll_adds"] = n_hll
+    res["hll_add_gkeys"] = round(n_hll / ms / 1e6, 3)
+    res["hll_add_hbm_frac"] = round(n_hll * 8 / (ms / 1e3) / 1e9 / peak, 4)
+    est = h.Estimate()
+    res["hll_estimate"] = est
+    res["hll_estimate_rel_err_vs_1e7"] = round(abs(est - 10_000_000) / 10_000_000, 5)
+    parts = [b2co.HyperLogLog(16) for _ in range(16)]
+    for i, p in enumerate(parts):
+        p.AddAsync(keys[i * (n_hll >> 4):(i + 1) * (n_hll >> 4)])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for p in parts[1:]:
+        parts[0].Merge(p)
+    res["hll_merge16_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+    res["hll_merge_equals_one_shot"] = bool(np.array_equal(parts[0].registers(), h.registers()))
+    return res
+
+
+def bloom_part(f_time, g, peak):
+    import torch
+    import b2co
+    res = {}
+    time_once = f_time
     nb, n = 1 << 22, 1 << 28
     f = b2co.BloomFilter(nb, key_dtype=torch.int64)
     adds = mix64_torch(counters(3 << 40, n, "torch"))
     absent = mix64_torch(counters(4 << 40, n // 2, "torch"))
-    g = torch.Generator(device="cuda").manual_seed(SEED + 7)
     q = torch.cat([adds[torch.randint(0, n, (n // 2,), generator=g, device="cuda")], absent])
     f.AddAsync(adds[: 1 << 20])  # warm-up launch
     f.Clear()
@@ -638,27 +686,6 @@ def bloom_hll_measurements(stream):
     res["bloom_no_false_negatives"] = bool(out[: n // 2].all().item())
     res["bloom_false_positive_rate"] = round(float(out[n // 2:].float().mean().item()), 6)
     del adds, absent, q, out, f
-
-    distinct = mix64_torch(counters(5 << 40, 10_000_000, "torch"))
-    keys = distinct[torch.randint(0, distinct.numel(), (1 << 30,), generator=g, device="cuda")]
-    h = b2co.HyperLogLog(16)
-    h.AddAsync(keys[: 1 << 20])
-    h.Clear()
-    ms = time_once(lambda: h.AddAsync(keys))
-    res["hll_add_gkeys"] = round((1 << 30) / ms / 1e6, 3)
-    res["hll_add_hbm_frac"] = round((1 << 30) * 8 / (ms / 1e3) / 1e9 / peak, 4)
-    est = h.Estimate()
-    res["hll_estimate"] = est
-    res["hll_estimate_rel_err_vs_1e7"] = round(abs(est - 10_000_000) / 10_000_000, 5)
-    parts = [b2co.HyperLogLog(16) for _ in range(16)]
-    for i, p in enumerate(parts):
-        p.AddAsync(keys[i * (1 << 26):(i + 1) * (1 << 26)])
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for p in parts[1:]:
-        parts[0].Merge(p)
-    res["hll_merge16_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
-    res["hll_merge_equals_one_shot"] = bool(np.array_equal(parts[0].registers(), h.registers()))
     return res
 
 
@@ -828,7 +855,8 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)", "impl": "reference",
         "config": {"workload": WORKLOAD, "capacity": cap, "unique_keys": unique, "queries_per_step": sample},
-        "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+        "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": threads, "kind": "port", "sample": desc,
+                         "cpu_model": cpu_model()},
         "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -850,8 +878,9 @@ def main():
     ap.add_argument("--queries-log2", type=int, default=27, help="queries per step 2^k (profiling: smaller)")
     ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
-    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll"],
+    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll", "hll"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
+    ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("warmup must be >= 3")
@@ -859,8 +888,8 @@ def main():
     REQ_CAPACITY, N_QUERIES = 1 << args.capacity_log2, 1 << args.queries_log2
     if args.only:
         import torch
-        fn = {"served": served_measurements, "batched": batched_measurements,
-              "bloom_hll": bloom_hll_measurements}[args.only]
+        fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,
+              "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2)}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
         run_reference(args)
