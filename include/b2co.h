@@ -106,6 +106,12 @@ int b2co_oa_destroy(b2co_oa_table* table);
 int b2co_oa_capacity(const b2co_oa_table* table, uint64_t* capacity);
 /* Raw device slots.  reference: static_map.h:604 Data(). */
 int b2co_oa_data(const b2co_oa_table* table, void** slots);
+/* The table's descriptor, sentinels masked to the key / payload widths and the
+ * current erased key included: what device code compiled by the caller needs
+ * to walk the slots (ForEach in include/b2co/for_each.cuh).  The reference's
+ * containers expose the same through their template parameters and
+ * constructor arguments (static_map.h:78-84). */
+int b2co_oa_describe(const b2co_oa_table* table, b2co_oa_desc* desc);
 /* reference: static_map.h:97 SetErasedKey (static_map.inl:59-66). */
 int b2co_oa_set_erased_key(b2co_oa_table* table, uint64_t erased_key_bits, b2co_stream stream);
 /* reference: static_map.h:318 Clear, :331 ClearAsync. */

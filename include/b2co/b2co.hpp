@@ -8,9 +8,11 @@
 // probing_scheme.h, storage.h, extent.h, pair.h).  The work itself runs in the
 // library's sm_100a kernels behind the C ABI (include/b2co.h).
 //
-// Compile-time policy types select run-time descriptor fields; functors that
-// cannot cross a C ABI (custom predicates, ForEach callbacks) are limited to
-// AlwaysTrue and the `uint8_t != 0` stencil.
+// Compile-time policy types select run-time descriptor fields.  Predicates
+// cannot cross a C ABI: they are limited to AlwaysTrue and the `uint8_t != 0`
+// stencil.  ForEach callbacks run in a kernel template compiled by the
+// caller's nvcc (b2co/for_each.cuh, pulled in when this header is compiled as
+// CUDA): StaticMap / StaticSet have ForEach / ForEachAsync only there.
 #pragma once
 
 #include <cstddef>
@@ -123,6 +125,12 @@ uint64_t bits_of(T v)
     std::memcpy(&b, &v, sizeof(T));
     return b;
 }
+
+#if defined(__CUDACC__)
+// Defined in b2co/for_each.cuh (T = void for a set).
+template <class CallbackOp, class Key, class T>
+void for_each_async(b2co_oa_table* t, void* keys, uint64_t n, void* args, cudaStream_t stream);
+#endif
 
 // Instance state of probing schemes / KeyEqual cannot reach the device
 // (open_addressing_impl.h:40-49 rejects non-default instances).
@@ -301,6 +309,21 @@ class StaticMap : public detail::OpenAddressing<Key, T, ExtentT, KeyEqual, Probi
         throw_on(b2co_oa_assign_if_async(this->handle(), v, reinterpret_cast<uint8_t const*>(st), static_cast<SizeType>(n), to_stream(s)));
     }
     ValueType* Data() const { return static_cast<ValueType*>(Base::Data()); }
+#if defined(__CUDACC__)
+    // reference: static_map.h:533-558 ForEach / ForEachAsync (static_map.inl:359-375).
+    template <typename CallbackOp>
+    void ForEach(void* keys, ExtentT keyNum, void* callbackArgs, cudaStream_t stream)
+    {
+        ForEachAsync<CallbackOp>(keys, keyNum, callbackArgs, stream);
+        throw_on(cudaStreamSynchronize(stream) == cudaSuccess ? B2CO_OK : B2CO_ECUDA);
+    }
+    template <typename CallbackOp>
+    void ForEachAsync(void* keys, ExtentT keyNum, void* callbackArgs, cudaStream_t stream)
+    {
+        detail::for_each_async<CallbackOp, Key, T>(this->handle(), keys, static_cast<SizeType>(keyNum), callbackArgs,
+                                                   stream);
+    }
+#endif
 
    private:
     Key emptyKey_;
@@ -323,6 +346,21 @@ class StaticSet : public detail::OpenAddressing<Key, Key, ExtentT, KeyEqual, Pro
     {}
     void SetErasedKey(Key erasedKey, cudaStream_t s) { this->SetErased(detail::bits_of(erasedKey), s); }
     Key* Data() const { return static_cast<Key*>(Base::Data()); }
+#if defined(__CUDACC__)
+    // reference: static_set.h ForEach / ForEachAsync (static_set.inl:247-262); the callback gets the key.
+    template <typename CallbackOp>
+    void ForEach(void* keys, ExtentT keyNum, void* callbackArgs, cudaStream_t stream)
+    {
+        ForEachAsync<CallbackOp>(keys, keyNum, callbackArgs, stream);
+        throw_on(cudaStreamSynchronize(stream) == cudaSuccess ? B2CO_OK : B2CO_ECUDA);
+    }
+    template <typename CallbackOp>
+    void ForEachAsync(void* keys, ExtentT keyNum, void* callbackArgs, cudaStream_t stream)
+    {
+        detail::for_each_async<CallbackOp, Key, void>(this->handle(), keys, static_cast<SizeType>(keyNum),
+                                                      callbackArgs, stream);
+    }
+#endif
 };
 
 // ---- dynamic_map.h ---------------------------------------------------------
@@ -509,3 +547,7 @@ class HyperLogLog {
 };
 
 }  // namespace b2co
+
+#if defined(__CUDACC__)
+#include "for_each.cuh"
+#endif

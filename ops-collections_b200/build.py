@@ -27,7 +27,8 @@ FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-re
 
 
 def _deps_mtime() -> float:
-    files = glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(REPO, "include", "*.h"))
+    files = (glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(REPO, "include", "*.h"))
+             + glob.glob(os.path.join(REPO, "include", "b2co", "*")))
     return max(os.path.getmtime(f) for f in files)
 
 

@@ -1,185 +1,13 @@
-// b2co_common.cuh -- hashing, probing and slot primitives shared by every
-// B200 kernel of the bulk-container library.
-//
-// Semantics follow the reference (ops-collections) exactly; each piece cites
-// the reference file it restates.  Everything here is __host__ __device__ so
-// the same code is unit-tested on the CPU.
+// b2co_common.cuh -- primitives shared by every B200 kernel of the
+// bulk-container library: the public hashing / probing / slot primitives
+// (include/b2co/device.cuh) plus the library-internal device helpers (slot
+// CAS, read-only and coherent slot loads, TMA bulk copies and mbarriers with
+// bounded waits).
 #pragma once
 
-#include <cstddef>
-#include <cstdint>
-#include <cuda_runtime.h>
-
-#include "../../include/b2co.h"
-
-#define B2CO_HD __host__ __device__ __forceinline__
+#include "../../include/b2co/device.cuh"
 
 namespace b2co {
-
-// ---------------------------------------------------------------------------
-// hashes over a key's object representation (little-endian, 4 or 8 bytes)
-// ---------------------------------------------------------------------------
-
-B2CO_HD uint32_t rotl32(uint32_t x, int r) { return (x << r) | (x >> (32 - r)); }
-B2CO_HD uint64_t rotl64(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
-
-// XXH32 for 4- and 8-byte inputs (include/detail/hash_functions/xxhash.h:52-175:
-// inputs shorter than 16 bytes take the seed+prime5 start and 4-byte lanes).
-template <int KB>
-B2CO_HD uint32_t xxh32(uint64_t key, uint32_t seed)
-{
-    constexpr uint32_t P1 = 0x9e3779b1u, P2 = 0x85ebca77u, P3 = 0xc2b2ae3du, P4 = 0x27d4eb2fu, P5 = 0x165667b1u;
-    uint32_t h = seed + P5 + uint32_t(KB);
-    h = rotl32(h + uint32_t(key) * P3, 17) * P4;
-    if constexpr (KB == 8) h = rotl32(h + uint32_t(key >> 32) * P3, 17) * P4;
-    h ^= h >> 15;
-    h *= P2;
-    h ^= h >> 13;
-    h *= P3;
-    h ^= h >> 16;
-    return h;
-}
-
-// XXH64 for 4- and 8-byte inputs (xxhash.h:184-326, fast paths :199-218).
-template <int KB>
-B2CO_HD uint64_t xxh64(uint64_t key, uint64_t seed)
-{
-    constexpr uint64_t P1 = 11400714785074694791ull, P2 = 14029467366897019727ull, P3 = 1609587929392839161ull,
-                       P4 = 9650029242287828579ull, P5 = 2870177450012600261ull;
-    uint64_t h = seed + P5 + uint64_t(KB);
-    if constexpr (KB == 8) {
-        h ^= rotl64(key * P2, 31) * P1;
-        h = rotl64(h, 27) * P1 + P4;
-    } else {
-        h ^= uint64_t(uint32_t(key)) * P1;
-        h = rotl64(h, 23) * P2 + P3;
-    }
-    h ^= h >> 33;
-    h *= P2;
-    h ^= h >> 29;
-    h *= P3;
-    h ^= h >> 32;
-    return h;
-}
-
-// MurmurHash3 finalizers with the seed xor-ed in first (hash_functions/utils.h:42-66).
-B2CO_HD uint32_t fmix32(uint32_t k, uint32_t seed)
-{
-    uint32_t h = k ^ seed;
-    h ^= h >> 16;
-    h *= 0x85ebca6bu;
-    h ^= h >> 13;
-    h *= 0xc2b2ae35u;
-    h ^= h >> 16;
-    return h;
-}
-B2CO_HD uint64_t fmix64(uint64_t k, uint64_t seed)
-{
-    uint64_t h = k ^ seed;
-    h ^= h >> 33;
-    h *= 0xff51afd7ed558ccdull;
-    h ^= h >> 33;
-    h *= 0xc4ceb9fe1a85ec53ull;
-    h ^= h >> 33;
-    return h;
-}
-
-// MurmurHash3_x86_32 for 4- and 8-byte inputs (hash_functions/murmurhash3.h:57-106).
-template <int KB>
-B2CO_HD uint32_t murmur3_32(uint64_t key, uint32_t seed)
-{
-    constexpr uint32_t c1 = 0xcc9e2d51u, c2 = 0x1b873593u;
-    uint32_t h = seed;
-#pragma unroll
-    for (int i = 0; i < KB / 4; ++i) {
-        uint32_t k = uint32_t(key >> (32 * i));
-        k *= c1;
-        k = rotl32(k, 15);
-        k *= c2;
-        h ^= k;
-        h = rotl32(h, 13);
-        h = h * 5 + 0xe6546b64u;
-    }
-    h ^= uint32_t(KB);
-    return fmix32(h, 0);
-}
-
-// The probing schemes cast the hash to the kernels' uint32 size type
-// (utility/math_utils.h:14-24 SanitizeHash).
-template <int KB>
-B2CO_HD uint32_t probe_hash(uint32_t kind, uint64_t key, uint32_t seed)
-{
-    switch (kind) {
-        case B2CO_HASH_MURMUR3_32: return murmur3_32<KB>(key, seed);
-        case B2CO_HASH_FMIX:
-            if constexpr (KB == 4) return fmix32(uint32_t(key), seed);
-            else return uint32_t(fmix64(key, seed));
-        case B2CO_HASH_XXH64: return uint32_t(xxh64<KB>(key, seed));
-        default: return xxh32<KB>(key, seed);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// exact 32-bit remainder by a runtime divisor (Lemire, Kaser, Kurz, "Faster
-// remainder by direct computation", 2019): M = floor((2^64-1)/d) + 1 and
-// a mod d = mulhi64(M * a, d) for every 32-bit a and d >= 1.
-// ---------------------------------------------------------------------------
-
-struct FastMod {
-    uint64_t m;
-    uint32_t d;
-};
-inline FastMod make_fastmod(uint32_t d) { return FastMod{~0ull / d + 1ull, d}; }
-
-B2CO_HD uint64_t mulhi64(uint64_t a, uint64_t b)
-{
-#ifdef __CUDA_ARCH__
-    return __umul64hi(a, b);
-#else
-    return uint64_t((unsigned __int128)a * b >> 64);
-#endif
-}
-B2CO_HD uint32_t fastmod(uint32_t a, FastMod f) { return uint32_t(mulhi64(f.m * uint64_t(a), f.d)); }
-
-// ---------------------------------------------------------------------------
-// probing: LinearProbing / DoubleHashing iterators
-// (detail/probing_scheme/probing_scheme_impl.inl:24-91, 116-128, 175-189)
-// ---------------------------------------------------------------------------
-
-struct ProbeParams {
-    uint32_t capacity;   // slots (a multiple of the bucket size)
-    uint32_t nbuckets;   // capacity / bucket size
-    FastMod mod_nb;      // % nbuckets
-    FastMod mod_nbm1;    // % (nbuckets - 1), double hashing only
-    uint32_t probing;    // B2CO_PROBE_*
-    uint32_t hash;       // B2CO_HASH_*
-};
-
-template <int KB, int B>
-B2CO_HD uint32_t probe_init(ProbeParams const& p, uint64_t key)
-{
-    return fastmod(probe_hash<KB>(p.hash, key, 0), p.mod_nb) * uint32_t(B);
-}
-
-// DoubleHashing's second hash is the same family seeded with 1 (probing_scheme.h:99).
-template <int KB, int B>
-B2CO_HD uint32_t probe_step(ProbeParams const& p, uint64_t key)
-{
-    if (p.probing == B2CO_PROBE_LINEAR) return uint32_t(B);
-    return (fastmod(probe_hash<KB>(p.hash, key, 1), p.mod_nbm1) + 1u) * uint32_t(B);
-}
-
-// Subtract before adding so the wrap never overflows (probing_scheme_impl.inl:76-84).
-B2CO_HD uint32_t probe_next(uint32_t idx, uint32_t step, uint32_t capacity)
-{
-    uint32_t rem = capacity - step;
-    return idx >= rem ? idx - rem : idx + step;
-}
-
-// ---------------------------------------------------------------------------
-// slot layouts: Pair<K,V> aligned to min(16, bitceil(sizeof K + sizeof V))
-// (pair.h:41, pair.inl:19-24), or a bare key for sets
-// ---------------------------------------------------------------------------
 
 // Device-side wait policy of kernels that wait on asynchronous copies: a wait
 // that exceeds `ns` nanoseconds stores kStatusTimeout into *status and the
@@ -190,68 +18,6 @@ struct WaitCtl {
     unsigned long long ns;
     unsigned int probe_timeout;  // test hook: the first wait is on a barrier nothing arrives on
 };
-
-struct alignas(16) U128 {
-    uint64_t lo, hi;
-};
-
-template <int KB, int VB>
-struct SlotT {
-    static constexpr int key_bytes = KB;
-    static constexpr int value_bytes = VB;
-    static constexpr bool is_set = VB == 0;
-    static constexpr int value_offset = VB == 0 ? 0 : ((KB + VB - 1) / VB) * VB;
-    static constexpr int bytes = VB == 0 ? KB : ((value_offset + VB) <= 8 ? 8 : 16);
-    // raw storage word of one slot
-    using Raw = typename std::conditional<bytes == 4, uint32_t,
-                typename std::conditional<bytes == 8, unsigned long long, U128>::type>::type;
-    static constexpr uint64_t kmask = KB == 8 ? ~0ull : 0xffffffffull;
-    static constexpr uint64_t vmask = VB == 8 ? ~0ull : (VB == 4 ? 0xffffffffull : 0ull);
-
-    B2CO_HD static uint64_t key(Raw r)
-    {
-        if constexpr (bytes == 16) return r.lo & kmask;
-        else return uint64_t(r) & kmask;
-    }
-    // Payload; a set's payload is the stored key (open_addressing_ref_impl.h:71-79).
-    B2CO_HD static uint64_t value(Raw r)
-    {
-        if constexpr (is_set) return key(r);
-        else if constexpr (bytes == 8) return uint64_t(r) >> 32;
-        else if constexpr (value_offset == 8) return r.hi & vmask;
-        else return r.lo >> 32;  // unreachable for supported layouts
-    }
-    B2CO_HD static Raw make(uint64_t k, uint64_t v)
-    {
-        if constexpr (bytes == 16) {
-            U128 r;
-            r.lo = k & kmask;
-            r.hi = v & vmask;
-            return r;
-        } else if constexpr (bytes == 8) {
-            if constexpr (is_set) return (unsigned long long)k;
-            else return (unsigned long long)((k & 0xffffffffull) | (v << 32));
-        } else {
-            return uint32_t(k);
-        }
-    }
-    // Same slot with the key replaced, every other byte kept.
-    B2CO_HD static Raw with_key(Raw r, uint64_t k)
-    {
-        if constexpr (bytes == 16) {
-            r.lo = (r.lo & ~kmask) | (k & kmask);
-            return r;
-        } else if constexpr (bytes == 8 && !is_set) {
-            return (unsigned long long)((uint64_t(r) & ~0xffffffffull) | (k & 0xffffffffull));
-        } else {
-            return Raw(k);
-        }
-    }
-};
-
-B2CO_HD bool raw_eq(uint32_t a, uint32_t b) { return a == b; }
-B2CO_HD bool raw_eq(unsigned long long a, unsigned long long b) { return a == b; }
-B2CO_HD bool raw_eq(U128 a, U128 b) { return a.lo == b.lo && a.hi == b.hi; }
 
 #ifdef __CUDACC__
 // Atomic compare-and-swap of a whole slot: 32-, 64- or 128-bit (the 128-bit form

@@ -270,6 +270,14 @@ int b2co_oa_data(b2co_oa_table const* t, void** slots)
     return B2CO_OK;
 }
 
+int b2co_oa_describe(b2co_oa_table const* t, b2co_oa_desc* desc)
+{
+    if (int st = check_table(t)) return st;
+    if (!desc) return fail(B2CO_EINVAL, "null output");
+    *desc = t->desc;
+    return B2CO_OK;
+}
+
 int b2co_oa_set_erased_key(b2co_oa_table* t, uint64_t erased, b2co_stream)
 {
     if (int st = check_table(t)) return st;
