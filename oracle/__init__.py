@@ -69,6 +69,10 @@ def lib():
             "orc_bloom_add": (None, [vp, u64, vp, u32, u64, u64]),
             "orc_bloom_contains": (None, [vp, u64, vp, u32, u64, u64, vp]),
             "orc_bloom_contains_parallel": (None, [vp, u64, vp, u32, u64, u64, vp, i32]),
+            "orc_bloom_policy_valid": (i32, [u32, u32]),
+            "orc_bloom_word_pattern": (u32, [u32, u32, u32]),
+            "orc_bloom_add_policy": (None, [vp, u64, u32, u32, vp, u32, u64, u64]),
+            "orc_bloom_contains_policy": (None, [vp, u64, u32, u32, vp, u32, u64, u64, vp, i32]),
             "orc_hll_add": (None, [vp, u32, vp, u32, u64]),
             "orc_hll_add_parallel": (None, [vp, u32, vp, u32, u64, i32]),
             "orc_hll_merge": (None, [vp, vp, u32]),
@@ -276,19 +280,30 @@ class Table:
 
 # ---- Bloom filter -----------------------------------------------------------
 
-def bloom_add(words: np.ndarray, num_blocks: int, keys: np.ndarray, seed: int = 0):
+def bloom_policy_valid(words_per_block: int, pattern_bits: int) -> bool:
+    return bool(lib().orc_bloom_policy_valid(words_per_block, pattern_bits))
+
+
+def bloom_word_patterns(words_per_block: int, pattern_bits: int, lower_hash: int):
+    """The per-word bit patterns one key sets (its 32-bit lower hash)."""
+    bpw = pattern_bits // words_per_block
+    return [lib().orc_bloom_word_pattern(w, bpw, lower_hash) for w in range(words_per_block)]
+
+
+def bloom_add(words: np.ndarray, num_blocks: int, keys: np.ndarray, seed: int = 0, words_per_block: int = 8,
+              pattern_bits: int = 8):
+    """Adds keys to a host word array of num_blocks * words_per_block uint32."""
     keys = np.ascontiguousarray(keys)
-    lib().orc_bloom_add(_p(words), num_blocks, _p(keys), keys.dtype.itemsize, len(keys), seed)
+    lib().orc_bloom_add_policy(_p(words), num_blocks, words_per_block, pattern_bits, _p(keys), keys.dtype.itemsize,
+                               len(keys), seed)
 
 
-def bloom_contains(words: np.ndarray, num_blocks: int, keys: np.ndarray, seed: int = 0, threads: int = 1):
+def bloom_contains(words: np.ndarray, num_blocks: int, keys: np.ndarray, seed: int = 0, threads: int = 1,
+                   words_per_block: int = 8, pattern_bits: int = 8):
     keys = np.ascontiguousarray(keys)
     out = np.empty(len(keys), dtype=np.uint8)
-    if threads == 1:
-        lib().orc_bloom_contains(_p(words), num_blocks, _p(keys), keys.dtype.itemsize, len(keys), seed, _p(out))
-    else:
-        lib().orc_bloom_contains_parallel(_p(words), num_blocks, _p(keys), keys.dtype.itemsize, len(keys), seed,
-                                          _p(out), threads)
+    lib().orc_bloom_contains_policy(_p(words), num_blocks, words_per_block, pattern_bits, _p(keys),
+                                    keys.dtype.itemsize, len(keys), seed, _p(out), threads)
     return out
 
 

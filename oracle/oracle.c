@@ -538,11 +538,19 @@ uint64_t orc_count(const orc_table* t, const void* keys, uint64_t n)
 /* Bloom filter                                                              */
 /* ------------------------------------------------------------------------ */
 
-/* First eight entries of the policy's salt table (bloom_filter_policy.h:170-178);
- * these are the split-block Bloom filter salts of the Parquet specification.  The
- * default policy (8 words per block, PatternBits 8) uses exactly these. */
-static const uint32_t k_salts[8] = {0x47b6137bu, 0x44974d91u, 0x8824ad5bu, 0xa2b7289du,
-                                    0x705495c7u, 0x2df1424bu, 0x9efc4947u, 0x5c6bfb31u};
+/* The policy's 64-entry salt table (bloom_filter_policy.h:170-178).  The first
+ * eight are the split-block Bloom filter salts of the Parquet specification and
+ * are all the default policy (8 words per block, PatternBits 8) uses; policies
+ * with more pattern bits take salt[w * bitsPerWord + b] for bit b of word w. */
+static const uint32_t k_salts[64] = {
+    0x47b6137bu, 0x44974d91u, 0x8824ad5bu, 0xa2b7289du, 0x705495c7u, 0x2df1424bu, 0x9efc4947u, 0x5c6bfb31u,
+    0xb24bcdffu, 0xb6843d6du, 0x6db04543u, 0x3a12efddu, 0xb0ddd463u, 0x8d22f6e7u, 0xb82f1e53u, 0x7db9f86bu,
+    0xc7afe639u, 0xfb135cd7u, 0x693256e1u, 0x9466d871u, 0x23d3d02fu, 0x6461d049u, 0x66a91621u, 0xbaa3006fu,
+    0x52fb8d99u, 0x3ea88b4fu, 0x0f470cfdu, 0xb1db79a5u, 0x9809fcd1u, 0xbced4445u, 0x2eb7c737u, 0x2cea6803u,
+    0x156f1955u, 0x8813c027u, 0xa26819f9u, 0x4c3b57bdu, 0x7df94487u, 0xb975e769u, 0xb8f20cb5u, 0x5c9e2e77u,
+    0x5fb1735fu, 0x3a6f759bu, 0x3c090923u, 0xfced424du, 0xa187a6a9u, 0x6f070a41u, 0x2c85233bu, 0x7e62258bu,
+    0x2771ef17u, 0x13bbf093u, 0x4ff059e5u, 0xe3ce3d0fu, 0xf1b4789fu, 0x9fbb6173u, 0x6a320cf5u, 0x1be2c481u,
+    0x7ba8222bu, 0x6fd619b3u, 0x7b1bbf0du, 0x8b8993adu, 0x448eca95u, 0x82ab09d9u, 0x2ce53909u, 0x4f548685u};
 
 static inline void bloom_locate(const void* keys, uint32_t kb, uint64_t i, uint64_t nblocks, uint64_t seed,
                                 uint32_t* block, uint32_t* lower)
@@ -554,47 +562,74 @@ static inline void bloom_locate(const void* keys, uint32_t kb, uint64_t i, uint6
     *lower = (uint32_t)h;
 }
 
-void orc_bloom_add(uint32_t* words, uint64_t nblocks, const void* keys, uint32_t kb, uint64_t n, uint64_t seed)
+/* Word w's pattern: bitsPerWord bits, bit b at (salt[w*bpw+b] * lower) >> 27
+ * for 32-bit words (WordPatternImpl, bloom_filter_policy.h:146-159). */
+uint32_t orc_bloom_word_pattern(uint32_t w, uint32_t bpw, uint32_t lower)
 {
+    uint32_t pat = 0;
+    for (uint32_t b = 0; b < bpw; ++b) pat |= 1u << ((k_salts[w * bpw + b] * lower) >> 27);
+    return pat;
+}
+
+int orc_bloom_policy_valid(uint32_t wpb, uint32_t pattern_bits)
+{
+    /* the static_asserts of the policy constructor (bloom_filter_policy.h:60-86), 32-bit words */
+    if (wpb == 0 || (wpb & (wpb - 1)) != 0 || wpb > 32) return 0;
+    if (pattern_bits < wpb || pattern_bits > 64 || pattern_bits > 32 * wpb || pattern_bits % wpb != 0) return 0;
+    return 1;
+}
+
+void orc_bloom_add_policy(uint32_t* words, uint64_t nblocks, uint32_t wpb, uint32_t pattern_bits, const void* keys,
+                          uint32_t kb, uint64_t n, uint64_t seed)
+{
+    uint32_t const bpw = pattern_bits / wpb;
     for (uint64_t i = 0; i < n; ++i) {
         uint32_t block, lower;
         bloom_locate(keys, kb, i, nblocks, seed, &block, &lower);
-        for (int w = 0; w < 8; ++w) words[(uint64_t)block * 8 + w] |= 1u << ((k_salts[w] * lower) >> 27);
+        for (uint32_t w = 0; w < wpb; ++w) words[(uint64_t)block * wpb + w] |= orc_bloom_word_pattern(w, bpw, lower);
     }
 }
 
-static inline uint8_t bloom_test(const uint32_t* words, uint32_t block, uint32_t lower)
+static inline uint8_t bloom_test(const uint32_t* words, uint32_t wpb, uint32_t bpw, uint32_t block, uint32_t lower)
 {
-    for (int w = 0; w < 8; ++w) {
-        uint32_t pat = 1u << ((k_salts[w] * lower) >> 27);
-        if ((words[(uint64_t)block * 8 + w] & pat) != pat) return 0;
+    for (uint32_t w = 0; w < wpb; ++w) {
+        uint32_t pat = orc_bloom_word_pattern(w, bpw, lower);
+        if ((words[(uint64_t)block * wpb + w] & pat) != pat) return 0;
     }
     return 1;
+}
+
+void orc_bloom_contains_policy(const uint32_t* words, uint64_t nblocks, uint32_t wpb, uint32_t pattern_bits,
+                               const void* keys, uint32_t kb, uint64_t n, uint64_t seed, uint8_t* out, int threads)
+{
+    uint32_t const bpw = pattern_bits / wpb;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(static, 65536) if (threads != 1)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        uint32_t block, lower;
+        bloom_locate(keys, kb, (uint64_t)i, nblocks, seed, &block, &lower);
+        out[i] = bloom_test(words, wpb, bpw, block, lower);
+    }
+    (void)threads;
+}
+
+void orc_bloom_add(uint32_t* words, uint64_t nblocks, const void* keys, uint32_t kb, uint64_t n, uint64_t seed)
+{
+    orc_bloom_add_policy(words, nblocks, 8, 8, keys, kb, n, seed);
 }
 
 void orc_bloom_contains(const uint32_t* words, uint64_t nblocks, const void* keys, uint32_t kb, uint64_t n,
                         uint64_t seed, uint8_t* out)
 {
-    for (uint64_t i = 0; i < n; ++i) {
-        uint32_t block, lower;
-        bloom_locate(keys, kb, i, nblocks, seed, &block, &lower);
-        out[i] = bloom_test(words, block, lower);
-    }
+    orc_bloom_contains_policy(words, nblocks, 8, 8, keys, kb, n, seed, out, 1);
 }
 
 void orc_bloom_contains_parallel(const uint32_t* words, uint64_t nblocks, const void* keys, uint32_t kb, uint64_t n,
                                  uint64_t seed, uint8_t* out, int threads)
 {
-#ifdef _OPENMP
-    if (threads > 0) omp_set_num_threads(threads);
-#pragma omp parallel for schedule(static, 65536)
-#endif
-    for (int64_t i = 0; i < (int64_t)n; ++i) {
-        uint32_t block, lower;
-        bloom_locate(keys, kb, (uint64_t)i, nblocks, seed, &block, &lower);
-        out[i] = bloom_test(words, block, lower);
-    }
-    (void)threads;
+    orc_bloom_contains_policy(words, nblocks, 8, 8, keys, kb, n, seed, out, threads);
 }
 
 /* ------------------------------------------------------------------------ */

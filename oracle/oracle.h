@@ -92,6 +92,15 @@ uint64_t orc_erase(orc_table* t, const void* keys, uint64_t n);
 uint64_t orc_count(const orc_table* t, const void* keys, uint64_t n);
 
 /* ---- Bloom filter (bloom_filter_policy.h:99-178, bloom_filter_impl.h:40-80) */
+/* Any BloomFilterPolicy with 32-bit words: wpb words per block, pattern_bits bits per key. */
+int orc_bloom_policy_valid(uint32_t wpb, uint32_t pattern_bits);
+uint32_t orc_bloom_word_pattern(uint32_t w, uint32_t bpw, uint32_t lower);
+void orc_bloom_add_policy(uint32_t* words, uint64_t num_blocks, uint32_t wpb, uint32_t pattern_bits, const void* keys,
+                          uint32_t key_bytes, uint64_t n, uint64_t seed);
+void orc_bloom_contains_policy(const uint32_t* words, uint64_t num_blocks, uint32_t wpb, uint32_t pattern_bits,
+                               const void* keys, uint32_t key_bytes, uint64_t n, uint64_t seed, uint8_t* out,
+                               int threads);
+/* The default policy (8 words per block, PatternBits 8). */
 void orc_bloom_add(uint32_t* words, uint64_t num_blocks, const void* keys, uint32_t key_bytes, uint64_t n,
                    uint64_t seed);
 void orc_bloom_contains(const uint32_t* words, uint64_t num_blocks, const void* keys, uint32_t key_bytes,

@@ -116,6 +116,50 @@ void ref_bloom_locate(int key_bytes, uint64_t key, uint64_t num_blocks, uint64_t
     if (key_bytes == 4) go(static_cast<uint32_t>(key)); else go(key);
 }
 
+}  // extern "C"
+
+namespace {
+template <uint32_t W, uint32_t P>
+int locate_policy(int key_bytes, uint64_t key, uint64_t num_blocks, uint64_t seed, uint32_t* block,
+                  uint32_t* patterns)
+{
+    auto go = [&](auto k) {
+        using K = decltype(k);
+        aclco::BloomFilterPolicy<K, aclco::xxhash_64<K>, uint32_t, W, P> pol{aclco::xxhash_64<K>{seed}};
+        uint64_t h = pol.HashKey(k);
+        *block = pol.BlockIndex(static_cast<uint32_t>(h >> 32), num_blocks);
+        for (uint32_t w = 0; w < W; ++w) patterns[w] = pol.WordPatternForLane(w, static_cast<uint32_t>(h));
+    };
+    if (key_bytes == 4) go(static_cast<uint32_t>(key)); else go(key);
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+
+// Any of the policies the fixtures cover: block index and the W word patterns of one key.
+int ref_bloom_locate_policy(int key_bytes, uint64_t key, uint64_t num_blocks, uint64_t seed, uint32_t words_per_block,
+                            uint32_t pattern_bits, uint32_t* block, uint32_t* patterns)
+{
+#define B2CO_POLICY(W, P) \
+    if (words_per_block == W && pattern_bits == P) return locate_policy<W, P>(key_bytes, key, num_blocks, seed, block, patterns);
+    B2CO_POLICY(1, 1)
+    B2CO_POLICY(1, 32)
+    B2CO_POLICY(2, 2)
+    B2CO_POLICY(2, 64)
+    B2CO_POLICY(4, 4)
+    B2CO_POLICY(4, 16)
+    B2CO_POLICY(8, 8)
+    B2CO_POLICY(8, 16)
+    B2CO_POLICY(8, 64)
+    B2CO_POLICY(16, 16)
+    B2CO_POLICY(16, 48)
+    B2CO_POLICY(32, 32)
+    B2CO_POLICY(32, 64)
+#undef B2CO_POLICY
+    return -1;
+}
+
 uint64_t ref_hll_finalize(int precision, double z, int v)
 {
     return aclco::detail::hyperloglog::Finalizer(precision)(z, v);

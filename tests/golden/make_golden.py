@@ -37,6 +37,7 @@ def load_probe(ref: str):
         "ref_valid_capacity": (u64, [u64, i32, i32]),
         "ref_probe_walk": (None, [i32, i32, i32, i32, u64, u32, u32, C.c_void_p]),
         "ref_bloom_locate": (None, [i32, u64, u64, u64, C.c_void_p, C.c_void_p]),
+        "ref_bloom_locate_policy": (i32, [i32, u64, u64, u64, u32, u32, C.c_void_p, C.c_void_p]),
         "ref_hll_finalize": (u64, [i32, dbl, i32]),
         "ref_hll_points": (i32, [i32]), "ref_hll_raw": (dbl, [i32, i32]),
         "ref_hll_bias": (dbl, [i32, i32]), "ref_hll_threshold": (dbl, [i32]),
@@ -138,7 +139,29 @@ def bloom(L, rng):
                     L.ref_bloom_locate(kb, k, nb, seed, C.byref(blk), pat)
                     rows.append({"key_bytes": kb, "num_blocks": nb, "seed": seed, "key": k,
                                  "block": blk.value, "patterns": list(pat)})
-    return {"locate": rows}
+    # non-default policies (WordsPerBlock, PatternBits), from the reference's own
+    # BloomFilterPolicy template; a separate generator keeps the rows above and
+    # the sections after this one unchanged
+    prng = np.random.default_rng(4242)
+    policy_rows = []
+    for wpb, pbits in POLICIES:
+        for kb in (4, 8):
+            for nb in (1, 257, 1 << 20):
+                for seed in (0, 42):
+                    for k in edge_keys(prng, kb)[:12]:
+                        blk = C.c_uint32()
+                        pat = (C.c_uint32 * wpb)()
+                        assert L.ref_bloom_locate_policy(kb, k, nb, seed, wpb, pbits, C.byref(blk), pat) == 0
+                        policy_rows.append({"words_per_block": wpb, "pattern_bits": pbits, "key_bytes": kb,
+                                            "num_blocks": nb, "seed": seed, "key": k, "block": blk.value,
+                                            "patterns": list(pat)})
+    return {"locate": rows, "policies": policy_rows}
+
+
+# (WordsPerBlock, PatternBits) of the policy fixtures: every word count the
+# policy allows, one and several bits per word, up to the 64-entry salt table.
+POLICIES = [(1, 1), (1, 32), (2, 2), (2, 64), (4, 4), (4, 16), (8, 8), (8, 16), (8, 64), (16, 16), (16, 48),
+            (32, 32), (32, 64)]
 
 
 def hll(L, rng):

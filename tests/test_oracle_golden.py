@@ -92,6 +92,30 @@ def test_probe_walks_match_reference():
         assert walk == r["walk"], r
 
 
+def test_bloom_policies_match_reference():
+    """Non-default BloomFilterPolicy<Key, xxhash_64, uint32_t, WordsPerBlock, PatternBits>:
+    block index and every word pattern of the reference's own template, and the
+    oracle's add/contains on them (the 64-entry salt table is pinned here)."""
+    rows = load("bloom")["policies"]
+    assert {(r["words_per_block"], r["pattern_bits"]) for r in rows} >= {(1, 32), (2, 64), (8, 16), (16, 48), (32, 64)}
+    for r in rows:
+        wpb, pbits, kb, nb, seed, k = (r["words_per_block"], r["pattern_bits"], r["key_bytes"], r["num_blocks"],
+                                       r["seed"], r["key"])
+        assert oracle.bloom_policy_valid(wpb, pbits)
+        h = oracle.xxh64(kbytes(k, kb), seed)
+        assert ((h >> 32) * (nb & 0xffffffff)) >> 32 == r["block"]
+        assert oracle.bloom_word_patterns(wpb, pbits, h & 0xffffffff) == r["patterns"]
+        if nb <= 257:
+            keys = np.array([k], dtype=np.uint32 if kb == 4 else np.uint64)
+            words = np.zeros(wpb * nb, dtype=np.uint32)
+            oracle.bloom_add(words, nb, keys, seed, wpb, pbits)
+            blk = r["block"]
+            assert words[blk * wpb:(blk + 1) * wpb].tolist() == r["patterns"]
+            assert oracle.bloom_contains(words, nb, keys, seed, 1, wpb, pbits).tolist() == [1]
+    for bad in [(3, 3), (64, 64), (8, 4), (8, 12), (4, 80), (1, 33)]:
+        assert not oracle.bloom_policy_valid(*bad)
+
+
 def test_bloom_locate_matches_reference():
     salts = [0x47b6137b, 0x44974d91, 0x8824ad5b, 0xa2b7289d, 0x705495c7, 0x2df1424b, 0x9efc4947, 0x5c6bfb31]
     for r in load("bloom")["locate"]:
