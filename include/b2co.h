@@ -329,6 +329,17 @@ typedef struct b2co_bloom b2co_bloom;
 /* reference: include/bloom_filter.h:59-62, bloom_filter_lifecycle.inl:15-52
  * (numBlocks 0 -> EINVAL, > UINT32_MAX -> ERANGE). */
 int b2co_bloom_create(uint64_t num_blocks, uint32_t key_bytes, uint64_t seed, b2co_stream stream, b2co_bloom** out);
+/* Any BloomFilterPolicy<Key, xxhash_64<Key>, uint32_t, WordsPerBlock, PatternBits, ...>
+ * (bloom_filter_policy.h:42-181): blocks of words_per_block uint32 words
+ * (a power of two <= 32), pattern_bits bits per key spread evenly over the
+ * words (a multiple of words_per_block, <= min(64, 32 * words_per_block));
+ * other values -> EINVAL, where the reference fails to compile.  The layout
+ * and ConditionalAdd / EarlyExitContains parameters change how the reference
+ * distributes work, not the bits, so they have no counterpart here.
+ * b2co_bloom_create is (8, 8), which is also ArrowFilterPolicy (:211). */
+int b2co_bloom_create_policy(uint64_t num_blocks, uint32_t key_bytes, uint64_t seed, uint32_t words_per_block,
+                             uint32_t pattern_bits, b2co_stream stream, b2co_bloom** out);
+int b2co_bloom_policy(const b2co_bloom* filter, uint32_t* words_per_block, uint32_t* pattern_bits);
 int b2co_bloom_destroy(b2co_bloom* filter);
 int b2co_bloom_data(const b2co_bloom* filter, uint32_t** words);
 int b2co_bloom_num_blocks(const b2co_bloom* filter, uint64_t* num_blocks);

@@ -433,12 +433,39 @@ class DynamicMap {
 };
 
 // ---- bloom_filter.h --------------------------------------------------------
-template <class Key>
+// The reference's template parameters, in its order (bloom_filter_policy.h:42-48).
+// WordsPerBlock and PatternBits select the bits; the layout and
+// ConditionalAdd / EarlyExitContains parameters only steer the reference's work
+// distribution and are accepted for source compatibility.
+template <class Key, class Hash = xxhash_64<Key>, class Word = uint32_t, uint32_t WordsPerBlock = 32 / sizeof(Word),
+          uint32_t PatternBits = WordsPerBlock, uint32_t AddHorizontalLayout = WordsPerBlock,
+          uint32_t AddVerticalLayout = 1, uint32_t ContainsHorizontalLayout = 1,
+          uint32_t ContainsVerticalLayout = WordsPerBlock, bool ConditionalAdd = false, bool EarlyExitContains = false>
 struct BloomFilterPolicy {
-    constexpr BloomFilterPolicy(xxhash_64<Key> h = {}) : seed_{h.seed_} {}
+    static_assert(std::is_same<Word, uint32_t>::value, "BloomFilter currently supports uint32_t words only");
+    static_assert(WordsPerBlock != 0 && (WordsPerBlock & (WordsPerBlock - 1)) == 0 && WordsPerBlock <= 32,
+                  "WordsPerBlock must be a non-zero power of two not above 32");
+    static_assert(PatternBits >= WordsPerBlock && PatternBits <= 64 && PatternBits <= 32 * WordsPerBlock &&
+                      PatternBits % WordsPerBlock == 0,
+                  "PatternBits must be evenly distributed across the words and fit the salt table");
+    static_assert(WordsPerBlock % (AddHorizontalLayout * AddVerticalLayout) == 0 &&
+                      WordsPerBlock % (ContainsHorizontalLayout * ContainsVerticalLayout) == 0,
+                  "layouts must evenly divide WordsPerBlock");
+    using KeyType = Key;
+    using Hasher = Hash;
+    using WordType = Word;
+    static constexpr uint32_t wordsPerBlock = WordsPerBlock;
+    static constexpr uint32_t patternBits = PatternBits;
+    constexpr BloomFilterPolicy(Hash h = {}) : seed_{h.seed_} {}
     constexpr bool operator==(BloomFilterPolicy const& o) const { return seed_ == o.seed_; }
     uint64_t seed_;
 };
+
+template <class Hash, class Word, uint32_t WordsPerBlock>
+using DefaultFilterPolicy = BloomFilterPolicy<typename Hash::ArgumentType, Hash, Word, WordsPerBlock>;
+
+template <class Key>
+using ArrowFilterPolicy = BloomFilterPolicy<Key, xxhash_64<Key>, uint32_t, 8, 8, 8, 1, 1, 8, false, false>;
 
 template <class Key, class ExtentT = Extent<std::size_t>, class Policy = BloomFilterPolicy<Key>>
 class BloomFilter {
@@ -449,7 +476,8 @@ class BloomFilter {
     using WordType = uint32_t;
     explicit BloomFilter(ExtentT numBlocks, Policy const& policy = Policy{}, cudaStream_t stream = nullptr)
     {
-        throw_on(b2co_bloom_create(static_cast<SizeType>(numBlocks), sizeof(Key), policy.seed_, to_stream(stream), &f_));
+        throw_on(b2co_bloom_create_policy(static_cast<SizeType>(numBlocks), sizeof(Key), policy.seed_,
+                                          Policy::wordsPerBlock, Policy::patternBits, to_stream(stream), &f_));
     }
     ~BloomFilter() { b2co_bloom_destroy(f_); }
     BloomFilter(BloomFilter const&) = delete;
@@ -492,7 +520,7 @@ class BloomFilter {
         throw_on(b2co_bloom_num_blocks(f_, &n));
         return ExtentT(SizeType(n));
     }
-    SizeType NumWords() const { return SizeType(static_cast<SizeType>(BlockExtent()) * 8); }
+    SizeType NumWords() const { return SizeType(static_cast<SizeType>(BlockExtent()) * Policy::wordsPerBlock); }
     std::size_t SizeBytes() const { return std::size_t(NumWords()) * sizeof(WordType); }
 
    private:

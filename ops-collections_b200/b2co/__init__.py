@@ -631,17 +631,22 @@ class DynamicMap:
 
 
 class BloomFilter:
-    """BloomFilter<Key> with the default policy (include/bloom_filter.h:37-39)."""
+    """BloomFilter<Key, Extent, BloomFilterPolicy<Key, xxhash_64<Key>, uint32_t,
+    WordsPerBlock, PatternBits>> (include/bloom_filter.h:37-39,
+    bloom_filter_policy.h:42-181); the defaults (8, 8) are the reference's
+    default policy and ArrowFilterPolicy."""
 
-    def __init__(self, num_blocks, key_dtype=None, seed=0, stream=None):
+    def __init__(self, num_blocks, key_dtype=None, seed=0, stream=None, words_per_block=8, pattern_bits=8):
         import torch
         key_dtype = key_dtype or torch.uint64
         self.key_bytes = _dtype_bytes(key_dtype)
         h = C.c_void_p()
-        _call("b2co_bloom_create", C.c_uint64(num_blocks), C.c_uint32(self.key_bytes), C.c_uint64(seed),
-              _stream(stream), C.byref(h))
+        _call("b2co_bloom_create_policy", C.c_uint64(num_blocks), C.c_uint32(self.key_bytes), C.c_uint64(seed),
+              C.c_uint32(words_per_block), C.c_uint32(pattern_bits), _stream(stream), C.byref(h))
         self._h = h
         self.num_blocks = num_blocks
+        self.words_per_block = words_per_block
+        self.pattern_bits = pattern_bits
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -655,8 +660,8 @@ class BloomFilter:
         return p.value
 
     def words(self) -> np.ndarray:
-        """The filter's words copied to the host (uint32, 8 per block)."""
-        return _device_bytes(self.Data(), self.num_blocks * 32).view(np.uint32)
+        """The filter's words copied to the host (uint32, words_per_block per block)."""
+        return _device_bytes(self.Data(), self.num_blocks * self.words_per_block * 4).view(np.uint32)
 
     def Clear(self, stream=None):
         _call("b2co_bloom_clear", self._h, _stream(stream))

@@ -1,14 +1,16 @@
-// bloom.cu -- BloomFilter<Key> with the reference's default policy
-// (bloom_filter_policy.h:54-181): 256-bit blocks of 8 uint32 words, xxh64 of
-// the key, block = mulhi32(upper hash, numBlocks), one bit per word at
-// (salt[w] * lower hash) >> 27.
+// bloom.cu -- BloomFilter<Key> with any BloomFilterPolicy of 32-bit words
+// (bloom_filter_policy.h:42-181): blocks of W uint32 words, xxh64 of the key,
+// block = mulhi32(upper hash, numBlocks), PatternBits / W bits per word, bit b
+// of word w at (salt[w * bitsPerWord + b] * lower hash) >> 27.
 //
-// B200 design: a block is exactly one 32-byte L2 sector.  Add issues the
-// block's 8 word bits as four 64-bit atomic ORs that need no return value
-// (RED), all to that one sector; lanes of a warp that hit the same block are
-// merged first (match_any) so each distinct block takes one set of REDs.
-// Contains reads the sector with two 16-byte loads.  Merge/Intersect stream
-// 16 bytes per lane.
+// B200 design for the default policy (W = 8, one bit per word): a block is
+// exactly one 32-byte L2 sector.  Add issues the block's 8 word bits as four
+// 64-bit atomic ORs that need no return value (RED), all to that one sector;
+// lanes of a warp that hit the same block are merged first (match_any) so each
+// distinct block takes one set of REDs.  Contains reads the sector with two
+// 16-byte loads.  Other policies run one key per thread: W/2 64-bit REDs (one
+// 32-bit RED for W = 1) and vector loads of the block.  Merge/Intersect stream
+// 16 bytes per lane (4 when the word count is not a multiple of 4).
 #include <new>
 
 #include "b2co_host.h"
@@ -17,10 +19,19 @@ using namespace b2co;
 
 namespace {
 
-// Split-block Bloom filter salts of the Parquet specification; the reference's
-// salt table starts with these eight (bloom_filter_policy.h:170-178).
-__constant__ uint32_t kSalts[8] = {0x47b6137bu, 0x44974d91u, 0x8824ad5bu, 0xa2b7289du,
-                                   0x705495c7u, 0x2df1424bu, 0x9efc4947u, 0x5c6bfb31u};
+// The policy's 64-entry salt table (bloom_filter_policy.h:170-178).  The first
+// eight are the split-block Bloom filter salts of the Parquet specification,
+// all the default policy uses; a policy with bitsPerWord bits per word takes
+// salt[w * bitsPerWord + b] for bit b of word w.
+__constant__ uint32_t kSalts[64] = {
+    0x47b6137bu, 0x44974d91u, 0x8824ad5bu, 0xa2b7289du, 0x705495c7u, 0x2df1424bu, 0x9efc4947u, 0x5c6bfb31u,
+    0xb24bcdffu, 0xb6843d6du, 0x6db04543u, 0x3a12efddu, 0xb0ddd463u, 0x8d22f6e7u, 0xb82f1e53u, 0x7db9f86bu,
+    0xc7afe639u, 0xfb135cd7u, 0x693256e1u, 0x9466d871u, 0x23d3d02fu, 0x6461d049u, 0x66a91621u, 0xbaa3006fu,
+    0x52fb8d99u, 0x3ea88b4fu, 0x0f470cfdu, 0xb1db79a5u, 0x9809fcd1u, 0xbced4445u, 0x2eb7c737u, 0x2cea6803u,
+    0x156f1955u, 0x8813c027u, 0xa26819f9u, 0x4c3b57bdu, 0x7df94487u, 0xb975e769u, 0xb8f20cb5u, 0x5c9e2e77u,
+    0x5fb1735fu, 0x3a6f759bu, 0x3c090923u, 0xfced424du, 0xa187a6a9u, 0x6f070a41u, 0x2c85233bu, 0x7e62258bu,
+    0x2771ef17u, 0x13bbf093u, 0x4ff059e5u, 0xe3ce3d0fu, 0xf1b4789fu, 0x9fbb6173u, 0x6a320cf5u, 0x1be2c481u,
+    0x7ba8222bu, 0x6fd619b3u, 0x7b1bbf0du, 0x8b8993adu, 0x448eca95u, 0x82ab09d9u, 0x2ce53909u, 0x4f548685u};
 
 template <int KB>
 __device__ __forceinline__ void locate(uint64_t key, uint64_t seed, uint32_t nblocks, uint32_t& block, uint32_t& lower)
@@ -97,6 +108,88 @@ __global__ void __launch_bounds__(256) k_bloom_contains(uint32_t const* words, u
     }
 }
 
+// ---- any other policy: W words per block, bpw bits per word ------------------
+
+__device__ __forceinline__ uint32_t policy_pattern(uint32_t w, uint32_t bpw, uint32_t lower)
+{
+    uint32_t pat = 0;
+    for (uint32_t b = 0; b < bpw; ++b) pat |= 1u << ((kSalts[w * bpw + b] * lower) >> 27);
+    return pat;
+}
+
+template <int KB, int W>
+__global__ void __launch_bounds__(256) k_bloom_add_policy(uint32_t* words, uint32_t nblocks, uint32_t bpw,
+                                                          uint64_t seed, void const* keys, uint8_t const* stencil,
+                                                          uint64_t n)
+{
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (stencil && !stencil[i]) continue;
+        uint32_t block, lower;
+        locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower);
+        uint32_t* blk = words + uint64_t(block) * W;
+        if constexpr (W == 1) {
+            atomicOr(blk, policy_pattern(0, bpw, lower));
+        } else {  // a block of W >= 2 words starts on an 8-byte boundary: 64-bit REDs
+#pragma unroll
+            for (int q = 0; q < W / 2; ++q)
+                atomicOr(reinterpret_cast<unsigned long long*>(blk) + q,
+                         (unsigned long long)policy_pattern(2 * q, bpw, lower) |
+                             ((unsigned long long)policy_pattern(2 * q + 1, bpw, lower) << 32));
+        }
+    }
+}
+
+template <int W>
+__device__ __forceinline__ void load_block(uint32_t const* blk, uint32_t (&w)[W])
+{
+    if constexpr (W % 4 == 0) {
+#pragma unroll
+        for (int q = 0; q < W / 4; ++q) {
+            uint4 v = __ldg(reinterpret_cast<uint4 const*>(blk) + q);
+            w[4 * q] = v.x, w[4 * q + 1] = v.y, w[4 * q + 2] = v.z, w[4 * q + 3] = v.w;
+        }
+    } else if constexpr (W == 2) {
+        uint2 v = __ldg(reinterpret_cast<uint2 const*>(blk));
+        w[0] = v.x, w[1] = v.y;
+    } else {
+        w[0] = __ldg(blk);
+    }
+}
+
+template <int KB, int W>
+__global__ void __launch_bounds__(256) k_bloom_contains_policy(uint32_t const* words, uint32_t nblocks, uint32_t bpw,
+                                                               uint64_t seed, void const* keys, uint8_t const* stencil,
+                                                               uint8_t* out, uint64_t n)
+{
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint8_t r = 0;
+        if (!stencil || stencil[i]) {
+            uint32_t block, lower;
+            locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower);
+            uint32_t w[W];
+            load_block<W>(words + uint64_t(block) * W, w);
+            bool all = true;
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                uint32_t const pat = policy_pattern(j, bpw, lower);
+                all &= (w[j] & pat) == pat;
+            }
+            r = all;
+        }
+        out[i] = r;
+    }
+}
+
+template <int OP>  // 0 = or, 1 = and; filters whose word count is not a multiple of 4
+__global__ void __launch_bounds__(256) k_bloom_combine32(uint32_t* dst, uint32_t const* src, uint64_t n)
+{
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        dst[i] = OP == 0 ? (dst[i] | __ldg(src + i)) : (dst[i] & __ldg(src + i));
+}
+
 template <int OP>  // 0 = or, 1 = and
 __global__ void __launch_bounds__(256) k_bloom_combine(uint4* dst, uint4 const* src, uint64_t n16)
 {
@@ -118,6 +211,10 @@ struct b2co_bloom {
     uint64_t num_blocks = 0;
     uint32_t key_bytes = 0;
     uint64_t seed = 0;
+    uint32_t wpb = 8;           // WordsPerBlock
+    uint32_t pattern_bits = 8;  // PatternBits
+    uint64_t num_words() const { return num_blocks * wpb; }
+    bool default_policy() const { return wpb == 8 && pattern_bits == 8; }
 };
 
 namespace {
@@ -135,8 +232,46 @@ int check_pair(b2co_bloom const* a, b2co_bloom const* b, char const* op)
     if (int st = check(b)) return st;
     if (a->num_blocks != b->num_blocks)
         return fail(B2CO_EINVAL, std::string("BloomFilter::") + op + ": filters have different block extents");
-    if (a->seed != b->seed || a->key_bytes != b->key_bytes)
+    if (a->seed != b->seed || a->key_bytes != b->key_bytes || a->wpb != b->wpb || a->pattern_bits != b->pattern_bits)
         return fail(B2CO_EINVAL, std::string("BloomFilter::") + op + ": filters have different policies");
+    return B2CO_OK;
+}
+
+template <int KB>
+int launch_add_policy(b2co_bloom* f, void const* keys, uint8_t const* stencil, uint64_t n, cudaStream_t s)
+{
+    void (*k)(uint32_t*, uint32_t, uint32_t, uint64_t, void const*, uint8_t const*, uint64_t) = nullptr;
+    switch (f->wpb) {
+        case 1: k = k_bloom_add_policy<KB, 1>; break;
+        case 2: k = k_bloom_add_policy<KB, 2>; break;
+        case 4: k = k_bloom_add_policy<KB, 4>; break;
+        case 8: k = k_bloom_add_policy<KB, 8>; break;
+        case 16: k = k_bloom_add_policy<KB, 16>; break;
+        default: k = k_bloom_add_policy<KB, 32>; break;
+    }
+    k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks),
+                                                           f->pattern_bits / f->wpb, f->seed, keys, stencil, n);
+    B2CO_CUDA(cudaGetLastError());
+    return B2CO_OK;
+}
+
+template <int KB>
+int launch_contains_policy(b2co_bloom* f, void const* keys, uint8_t const* stencil, uint8_t* out, uint64_t n,
+                           cudaStream_t s)
+{
+    void (*k)(uint32_t const*, uint32_t, uint32_t, uint64_t, void const*, uint8_t const*, uint8_t*, uint64_t) =
+        nullptr;
+    switch (f->wpb) {
+        case 1: k = k_bloom_contains_policy<KB, 1>; break;
+        case 2: k = k_bloom_contains_policy<KB, 2>; break;
+        case 4: k = k_bloom_contains_policy<KB, 4>; break;
+        case 8: k = k_bloom_contains_policy<KB, 8>; break;
+        case 16: k = k_bloom_contains_policy<KB, 16>; break;
+        default: k = k_bloom_contains_policy<KB, 32>; break;
+    }
+    k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks),
+                                                           f->pattern_bits / f->wpb, f->seed, keys, stencil, out, n);
+    B2CO_CUDA(cudaGetLastError());
     return B2CO_OK;
 }
 
@@ -147,6 +282,8 @@ int add_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_s
     if (!keys) return fail(B2CO_EINVAL, "BloomFilter::Add: keys must not be null when keyNum is non-zero");
     if (use_stencil && !stencil)
         return fail(B2CO_EINVAL, "BloomFilter::AddIf: stencil must not be null when keyNum is non-zero");
+    if (!f->default_policy())
+        return f->key_bytes == 8 ? launch_add_policy<8>(f, keys, stencil, n, s) : launch_add_policy<4>(f, keys, stencil, n, s);
     void (*k)(uint32_t*, uint32_t, uint64_t, void const*, uint8_t const*, uint64_t) =
         f->key_bytes == 8 ? k_bloom_add<8> : k_bloom_add<4>;
     k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks), f->seed, keys, stencil,
@@ -164,6 +301,9 @@ int contains_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool 
     if (!out) return fail(B2CO_EINVAL, "BloomFilter::Contains: outputValues must not be null when keyNum is non-zero");
     if (use_stencil && !stencil)
         return fail(B2CO_EINVAL, "BloomFilter::ContainsIf: stencil must not be null when keyNum is non-zero");
+    if (!f->default_policy())
+        return f->key_bytes == 8 ? launch_contains_policy<8>(f, keys, stencil, out, n, s)
+                                 : launch_contains_policy<4>(f, keys, stencil, out, n, s);
     void (*k)(uint32_t const*, uint32_t, uint64_t, void const*, uint8_t const*, uint8_t*, uint64_t) =
         f->key_bytes == 8 ? k_bloom_contains<8> : k_bloom_contains<4>;
     k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks), f->seed, keys, stencil,
@@ -177,10 +317,16 @@ int combine(b2co_bloom* f, b2co_bloom const* o, cudaStream_t s, char const* name
 {
     if (int st = check_pair(f, o, name)) return st;
     if (f == o) return B2CO_OK;
-    uint64_t n16 = f->num_blocks * 2;
-    auto k = k_bloom_combine<OP>;
-    k<<<grid_for((void const*)k, 256, n16, 256), 256, 0, s>>>(reinterpret_cast<uint4*>(f->words),
-                                                              reinterpret_cast<uint4 const*>(o->words), n16);
+    uint64_t const nw = f->num_words();
+    if (nw % 4 == 0) {
+        uint64_t const n16 = nw / 4;
+        auto k = k_bloom_combine<OP>;
+        k<<<grid_for((void const*)k, 256, n16, 256), 256, 0, s>>>(reinterpret_cast<uint4*>(f->words),
+                                                                  reinterpret_cast<uint4 const*>(o->words), n16);
+    } else {
+        auto k = k_bloom_combine32<OP>;
+        k<<<grid_for((void const*)k, 256, nw, 256), 256, 0, s>>>(f->words, o->words, nw);
+    }
     B2CO_CUDA(cudaGetLastError());
     return B2CO_OK;
 }
@@ -197,18 +343,33 @@ extern "C" {
 
 int b2co_bloom_create(uint64_t num_blocks, uint32_t key_bytes, uint64_t seed, b2co_stream stream, b2co_bloom** out)
 {
+    return b2co_bloom_create_policy(num_blocks, key_bytes, seed, 8, 8, stream, out);
+}
+
+int b2co_bloom_create_policy(uint64_t num_blocks, uint32_t key_bytes, uint64_t seed, uint32_t words_per_block,
+                             uint32_t pattern_bits, b2co_stream stream, b2co_bloom** out)
+{
     if (!out) return fail(B2CO_EINVAL, "null output");
     *out = nullptr;
     if (num_blocks == 0) return fail(B2CO_EINVAL, "BloomFilter: numBlocks must be greater than zero");
     if (num_blocks > 0xffffffffull)
         return fail(B2CO_ERANGE, "BloomFilter: numBlocks exceeds the supported block-index range");
     if (key_bytes != 4 && key_bytes != 8) return fail(B2CO_EINVAL, "BloomFilter: key_bytes must be 4 or 8");
+    // the policy constructor's static_asserts (bloom_filter_policy.h:60-86) for 32-bit words
+    uint32_t const w = words_per_block, p = pattern_bits;
+    if (w == 0 || (w & (w - 1)) != 0 || w > 32)
+        return fail(B2CO_EINVAL, "BloomFilter: WordsPerBlock must be a power of two not above 32");
+    if (p < w || p > 64 || p > 32 * w || p % w != 0)
+        return fail(B2CO_EINVAL, "BloomFilter: PatternBits must be a multiple of WordsPerBlock in [WordsPerBlock, "
+                                 "min(64, 32 * WordsPerBlock)]");
     auto* f = new (std::nothrow) b2co_bloom;
     if (!f) return fail(B2CO_ENOMEM, "host allocation failed");
     f->num_blocks = num_blocks;
     f->key_bytes = key_bytes;
     f->seed = seed;
-    cudaError_t e = cudaMalloc(&f->words, num_blocks * 32);
+    f->wpb = w;
+    f->pattern_bits = p;
+    cudaError_t e = cudaMalloc(&f->words, f->num_words() * 4);
     if (e != cudaSuccess) {
         delete f;
         return cuda_fail(e, "BloomFilter allocation");
@@ -245,10 +406,19 @@ int b2co_bloom_num_blocks(b2co_bloom const* f, uint64_t* nb)
     return B2CO_OK;
 }
 
+int b2co_bloom_policy(b2co_bloom const* f, uint32_t* words_per_block, uint32_t* pattern_bits)
+{
+    if (int st = check(f)) return st;
+    if (!words_per_block || !pattern_bits) return fail(B2CO_EINVAL, "null output");
+    *words_per_block = f->wpb;
+    *pattern_bits = f->pattern_bits;
+    return B2CO_OK;
+}
+
 int b2co_bloom_clear_async(b2co_bloom* f, b2co_stream s)
 {
     if (int st = check(f)) return st;
-    B2CO_CUDA(cudaMemsetAsync(f->words, 0, f->num_blocks * 32, cs(s)));
+    B2CO_CUDA(cudaMemsetAsync(f->words, 0, f->num_words() * 4, cs(s)));
     return B2CO_OK;
 }
 

@@ -157,6 +157,28 @@ int main()
         expect_throw<std::length_error>([&] { b2co::BloomFilter<uint64_t> big(b2co::Extent<size_t>{size_t(1) << 32}); });
     }
 
+    // ---- policy aliases (bloom_filter_policy.h:205-211, generalization_test.cpp:32-41) ----
+    {
+        static_assert(std::is_same<b2co::ArrowFilterPolicy<uint32_t>,
+                                   b2co::BloomFilterPolicy<uint32_t, b2co::xxhash_64<uint32_t>, uint32_t, 8, 8, 8, 1,
+                                                           1, 8, false, false>>::value,
+                      "ArrowFilterPolicy is the 8-word, 8-bit policy");
+        using P16 = b2co::DefaultFilterPolicy<b2co::xxhash_64<uint64_t>, uint32_t, 16>;
+        static_assert(P16::wordsPerBlock == 16 && P16::patternBits == 16, "DefaultFilterPolicy<..., 16>");
+        b2co::BloomFilter<uint64_t, b2co::Extent<size_t>, P16> f(b2co::Extent<size_t>{4096}, P16{}, stream);
+        CHECK(f.NumWords() == 4096 * 16);
+        std::vector<uint64_t> keys(50000);
+        for (auto& k : keys) k = gen();
+        DeviceBuffer<uint64_t> dk(keys);
+        DeviceBuffer<uint8_t> out(keys.size());
+        f.Add(dk.p, b2co::Extent<size_t>{keys.size()}, stream);
+        f.Contains(dk.p, b2co::Extent<size_t>{keys.size()}, out.p, stream);
+        for (auto v : out.download()) CHECK(v == 1);
+        using Seeded = b2co::BloomFilterPolicy<uint32_t, b2co::xxhash_64<uint32_t>, uint32_t, 8, 16, 1, 8, 1, 8, true, true>;
+        b2co::BloomFilter<uint32_t, b2co::Extent<size_t>, Seeded> g(b2co::Extent<size_t>{257}, Seeded{b2co::xxhash_64<uint32_t>{42}}, stream);
+        CHECK(g.NumWords() == 257 * 8);
+    }
+
     // ---- HyperLogLog<int64_t>: estimate within 3 standard errors ----
     {
         auto h = b2co::HyperLogLog<int64_t>::CreateWithSketchSizeKB(64, stream);

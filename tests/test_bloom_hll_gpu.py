@@ -75,6 +75,75 @@ def test_bloom_add_if_merge_intersect_and_errors():
     assert not a.words().any()
 
 
+POLICIES = [(1, 1), (1, 32), (2, 2), (2, 64), (4, 4), (4, 16), (8, 16), (8, 64), (16, 16), (16, 48), (32, 32),
+            (32, 64)]
+
+
+@pytest.mark.parametrize("policy", POLICIES, ids=lambda p: f"w{p[0]}p{p[1]}")
+@pytest.mark.parametrize("key_bytes", [4, 8])
+def test_bloom_policy_bit_exact(policy, key_bytes):
+    """Non-default BloomFilterPolicy (WordsPerBlock, PatternBits), as in the
+    reference's generalization_test.cpp: the bit array after Add and AddIf, the
+    results of Contains and ContainsIf, Merge and Intersect all equal the oracle."""
+    import b2co
+    import torch
+    wpb, pbits = policy
+    rng = np.random.default_rng(wpb * 100 + pbits + key_bytes)
+    kdt = np.uint32 if key_bytes == 4 else np.uint64
+    tdt = torch.int32 if key_bytes == 4 else torch.int64
+    vdt = np.int32 if key_bytes == 4 else np.int64
+    for nb, seed in [(257, 42), (1 << 16, 0)]:
+        n = 40000
+        keys = rng.integers(0, np.iinfo(kdt).max, size=n, dtype=np.uint64).astype(kdt)
+        keys[n // 2:n // 2 + 1000] = keys[:1000]  # repeated keys
+        f = b2co.BloomFilter(nb, key_dtype=tdt, seed=seed, words_per_block=wpb, pattern_bits=pbits)
+        st = (rng.random(n) < 0.6).astype(np.uint8)
+        f.Add(dev(keys[: n // 2].view(vdt)))
+        f.AddIf(dev(keys[n // 2:].view(vdt)), dev(st[n // 2:]))
+        words = np.zeros(nb * wpb, dtype=np.uint32)
+        oracle.bloom_add(words, nb, keys[: n // 2], seed, wpb, pbits)
+        oracle.bloom_add(words, nb, keys[n // 2:][st[n // 2:].astype(bool)], seed, wpb, pbits)
+        assert np.array_equal(f.words(), words)
+        q = np.concatenate([keys[::7], rng.integers(0, np.iinfo(kdt).max, size=20000, dtype=np.uint64).astype(kdt)])
+        out = torch.empty(len(q), dtype=torch.uint8, device="cuda")
+        f.Contains(dev(q.view(vdt)), out)
+        exp = oracle.bloom_contains(words, nb, q, seed, 1, wpb, pbits)
+        assert np.array_equal(out.cpu().numpy(), exp)
+        qs = (rng.random(len(q)) < 0.5).astype(np.uint8)
+        f.ContainsIf(dev(q.view(vdt)), dev(qs), out)
+        assert np.array_equal(out.cpu().numpy(), exp & qs)
+        g = b2co.BloomFilter(nb, key_dtype=tdt, seed=seed, words_per_block=wpb, pattern_bits=pbits)
+        other = keys[: n // 3][::-1].copy()
+        g.Add(dev(other.view(vdt)))
+        wg = np.zeros_like(words)
+        oracle.bloom_add(wg, nb, other, seed, wpb, pbits)
+        f.Merge(g)
+        assert np.array_equal(f.words(), words | wg)
+        f.Intersect(g)
+        assert np.array_equal(f.words(), (words | wg) & wg)
+        with pytest.raises(b2co.InvalidArgument):  # same blocks, different policy
+            f.Merge(b2co.BloomFilter(nb, key_dtype=tdt, seed=seed, words_per_block=wpb * 2 if wpb < 32 else 16,
+                                     pattern_bits=64))
+        f.Clear()
+        assert not f.words().any()
+
+
+def test_bloom_policy_arguments():
+    import b2co
+    import torch
+    for wpb, pbits in [(3, 3), (64, 64), (8, 4), (8, 12), (4, 80), (1, 33), (0, 8)]:
+        with pytest.raises(b2co.InvalidArgument):
+            b2co.BloomFilter(16, key_dtype=torch.int64, words_per_block=wpb, pattern_bits=pbits)
+    # the default filter and an explicit (8, 8) filter (ArrowFilterPolicy) are the same filter
+    keys = np.arange(1, 5001, dtype=np.int64) * 2654435761
+    a = b2co.BloomFilter(333, key_dtype=torch.int64)
+    b = b2co.BloomFilter(333, key_dtype=torch.int64, words_per_block=8, pattern_bits=8)
+    a.Add(dev(keys))
+    b.Add(dev(keys))
+    assert np.array_equal(a.words(), b.words())
+    a.Merge(b)
+
+
 @pytest.mark.parametrize("precision", [13, 14, 15, 16, 17, 18])
 @pytest.mark.parametrize("key_bytes", [4, 8])
 def test_hll_registers_bit_exact(precision, key_bytes):
