@@ -43,7 +43,8 @@ typedef enum {
     B2CO_ENOMEM = 3,   /* std::bad_alloc */
     B2CO_ECUDA = 4,    /* std::runtime_error: a CUDA call failed */
     B2CO_ETIMEOUT = 5, /* a bounded device-side wait expired (no reference counterpart) */
-    B2CO_ELOGIC = 6    /* std::logic_error: moved-from / storage-less object */
+    B2CO_ELOGIC = 6,   /* std::logic_error: moved-from / storage-less object */
+    B2CO_EOVERFLOW = 7 /* std::overflow_error: a result cannot be represented */
 } b2co_status;
 
 typedef enum { B2CO_HASH_XXH32 = 0, B2CO_HASH_MURMUR3_32 = 1, B2CO_HASH_FMIX = 2, B2CO_HASH_XXH64 = 3 } b2co_hash;
@@ -319,6 +320,83 @@ typedef struct {
 int b2co_server_get_stats_ex(b2co_server* server, b2co_server_stats_ex* stats);
 /* Finishes every submitted request, then stops the dispatcher. */
 int b2co_server_destroy(b2co_server* server);
+
+/* ===================================================================== */
+/* StaticMultiset<Key> / StaticMultimap<Key, Value>, Key and Value int32 or  */
+/* int64                                                                   */
+/* ===================================================================== */
+/* The reference's containers expose no slot layout (no Data()); results are
+ * defined by the stored entries and the reference's ordering rules, which
+ * these follow.  Capacities are exact element counts up to 2^31.  All calls
+ * are synchronous, like the reference's (include/static_multiset.h,
+ * include/static_multimap.h).  Stencils are uint8 (nonzero = selected). */
+typedef struct b2co_mset b2co_mset;
+/* reference: static_multiset.h:55 (capacity 0 -> EINVAL). */
+int b2co_mset_create(uint64_t capacity, uint32_t key_bytes, uint64_t empty_key_bits, b2co_stream stream,
+                     b2co_mset** out);
+int b2co_mset_destroy(b2co_mset* set);
+int b2co_mset_capacity(const b2co_mset* set, uint64_t* capacity);
+int b2co_mset_size(const b2co_mset* set, uint64_t* size);
+int b2co_mset_clear(b2co_mset* set, b2co_stream stream);
+/* reference: static_multiset.h:159-190 Insert / InsertIf: the earliest valid
+ * selected keys up to the remaining capacity are kept in input order;
+ * *failed = sentinel keys + selected keys beyond the capacity; a NULL key
+ * array with n > 0 reports n failed and changes nothing. */
+int b2co_mset_insert(b2co_mset* set, const void* keys, uint64_t n, b2co_stream stream, uint64_t* failed);
+int b2co_mset_insert_if(b2co_mset* set, const void* keys, const uint8_t* stencil, uint64_t n, b2co_stream stream,
+                        uint64_t* failed);
+/* reference: static_multiset.h:192-240 Contains(If) (u8), Find(If) (the key
+ * or the empty key), :242-260 CountEach / CountEachOuter (uint64, 0 -> 1). */
+int b2co_mset_contains(b2co_mset* set, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+int b2co_mset_contains_if(b2co_mset* set, const void* keys, const uint8_t* stencil, uint8_t* out, uint64_t n,
+                          b2co_stream stream);
+int b2co_mset_find(b2co_mset* set, const void* keys, void* out, uint64_t n, b2co_stream stream);
+int b2co_mset_find_if(b2co_mset* set, const void* keys, const uint8_t* stencil, void* out, uint64_t n,
+                      b2co_stream stream);
+int b2co_mset_count_each(b2co_mset* set, const void* keys, uint64_t* out, uint64_t n, b2co_stream stream);
+int b2co_mset_count_each_outer(b2co_mset* set, const void* keys, uint64_t* out, uint64_t n, b2co_stream stream);
+/* reference: :290-294 Count (n * Size() not representable -> EOVERFLOW). */
+int b2co_mset_count(b2co_mset* set, const void* keys, uint64_t n, b2co_stream stream, uint64_t* total);
+/* reference: :296-321 Retrieve: per query in order, `count` (query, stored
+ * key) pairs; total > out_capacity -> ERANGE with nothing written. */
+int b2co_mset_retrieve(b2co_mset* set, const void* keys, uint64_t n, void* probe_out, void* match_out,
+                       uint64_t out_capacity, b2co_stream stream, uint64_t* written);
+/* reference: :322-343 RetrieveAll: every stored key in accepted insertion order. */
+int b2co_mset_retrieve_all(b2co_mset* set, void* out, uint64_t out_capacity, b2co_stream stream, uint64_t* written);
+
+typedef struct b2co_mmap b2co_mmap;
+/* reference: static_multimap.h:402-410 (capacity 0 -> EINVAL). */
+int b2co_mmap_create(uint64_t capacity, uint32_t key_bytes, uint32_t value_bytes, uint64_t empty_key_bits,
+                     uint64_t empty_value_bits, b2co_stream stream, b2co_mmap** out);
+int b2co_mmap_destroy(b2co_mmap* map);
+int b2co_mmap_capacity(const b2co_mmap* map, uint64_t* capacity);
+int b2co_mmap_size(const b2co_mmap* map, uint64_t* size);
+int b2co_mmap_clear(b2co_mmap* map, b2co_stream stream);
+/* reference: static_multimap.h:430-460, :288-399 Insert / InsertIf over
+ * Pair<Key, Value>: every selected pair is validated first (a sentinel key or
+ * value -> EINVAL, nothing inserted); the earliest selected pairs up to the
+ * remaining capacity are kept, duplicates included; *failed = selected pairs
+ * not admitted. */
+int b2co_mmap_insert(b2co_mmap* map, const void* pairs, uint64_t n, b2co_stream stream, uint64_t* failed);
+int b2co_mmap_insert_if(b2co_mmap* map, const void* pairs, const uint8_t* stencil, uint64_t n, b2co_stream stream,
+                        uint64_t* failed);
+/* reference: :461-480 Contains(If) (u8), Find(If) (the smallest value stored
+ * under the key, else the empty value; static_multimap_ref.h QueryImpl). */
+int b2co_mmap_contains(b2co_mmap* map, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+int b2co_mmap_contains_if(b2co_mmap* map, const void* keys, const uint8_t* stencil, uint8_t* out, uint64_t n,
+                          b2co_stream stream);
+int b2co_mmap_find(b2co_mmap* map, const void* keys, void* out, uint64_t n, b2co_stream stream);
+int b2co_mmap_find_if(b2co_mmap* map, const void* keys, const uint8_t* stencil, void* out, uint64_t n,
+                      b2co_stream stream);
+/* reference: :481-492 Count (EOVERFLOW as for the multiset). */
+int b2co_mmap_count(b2co_mmap* map, const void* keys, uint64_t n, b2co_stream stream, uint64_t* total);
+/* reference: :493-510 Retrieve: per query in order, its values ascending;
+ * total > out_capacity -> ERANGE with nothing written. */
+int b2co_mmap_retrieve(b2co_mmap* map, const void* keys, uint64_t n, void* key_out, void* value_out,
+                       uint64_t out_capacity, b2co_stream stream, uint64_t* written);
+/* reference: :512-553 RetrieveAll: all pairs, in accepted insertion order. */
+int b2co_mmap_retrieve_all(b2co_mmap* map, void* key_out, void* value_out, uint64_t out_capacity,
+                           b2co_stream stream, uint64_t* written);
 
 /* ===================================================================== */
 /* BloomFilter<Key>, default policy (8 x uint32 words per block, xxh64)     */

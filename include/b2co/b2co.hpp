@@ -40,6 +40,7 @@ inline void throw_on(int status)
         case B2CO_ERANGE: throw std::length_error(msg);
         case B2CO_ENOMEM: throw std::bad_alloc();
         case B2CO_ELOGIC: throw std::logic_error(msg);
+        case B2CO_EOVERFLOW: throw std::overflow_error(msg);
         default: throw std::runtime_error(msg);
     }
 }

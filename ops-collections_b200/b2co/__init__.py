@@ -25,7 +25,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libb2co.so")
 
-OK, EINVAL, ERANGE, ENOMEM, ECUDA, ETIMEOUT, ELOGIC = range(7)
+OK, EINVAL, ERANGE, ENOMEM, ECUDA, ETIMEOUT, ELOGIC, EOVERFLOW = range(8)
 HASH_XXH32, HASH_MURMUR3_32, HASH_FMIX, HASH_XXH64 = range(4)
 PROBE_LINEAR, PROBE_DOUBLE = 0, 1
 IAF_RACE, IAF_FIRST_WINS = 0, 1
@@ -63,8 +63,12 @@ class LogicError(B2coError, RuntimeError):
     status = ELOGIC
 
 
+class OverflowError_(B2coError, OverflowError):
+    status = EOVERFLOW
+
+
 _EXC = {EINVAL: InvalidArgument, ERANGE: LengthError, ENOMEM: BadAlloc, ECUDA: CudaError,
-        ETIMEOUT: TimeoutError_, ELOGIC: LogicError}
+        ETIMEOUT: TimeoutError_, ELOGIC: LogicError, EOVERFLOW: OverflowError_}
 
 
 class OaDesc(C.Structure):
@@ -628,6 +632,148 @@ class DynamicMap:
 
     def Clear(self, stream=None):
         _call("b2co_dmap_clear", self._h, _stream(stream))
+
+
+class StaticMultiset:
+    """StaticMultiset<Key> (include/static_multiset.h), Key int32 or int64;
+    device tensors in and out; synchronous like the reference."""
+
+    def __init__(self, capacity, empty_key, key_dtype=None, stream=None):
+        import torch
+        key_dtype = key_dtype or torch.int64
+        self.key_bytes = _dtype_bytes(key_dtype)
+        h = C.c_void_p()
+        _call("b2co_mset_create", C.c_uint64(capacity), C.c_uint32(self.key_bytes),
+              C.c_uint64(_bits(empty_key, self.key_bytes)), _stream(stream), C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_mset_destroy(h)
+            self._h = None
+
+    def _u64(self, name, *args):
+        v = C.c_uint64()
+        _call(name, self._h, *args, C.byref(v))
+        return v.value
+
+    def Capacity(self):
+        return self._u64("b2co_mset_capacity")
+
+    def Size(self, stream=None):
+        return self._u64("b2co_mset_size")
+
+    def Clear(self, stream=None):
+        _call("b2co_mset_clear", self._h, _stream(stream))
+
+    def Insert(self, keys, n=None, stream=None):
+        return self._u64("b2co_mset_insert", _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def InsertIf(self, keys, stencil, n=None, stream=None):
+        return self._u64("b2co_mset_insert_if", _ptr(keys), _ptr(stencil), C.c_uint64(_OaBase._n(keys, n)),
+                         _stream(stream))
+
+    def Contains(self, keys, output, n=None, stream=None):
+        _call("b2co_mset_contains", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def ContainsIf(self, keys, stencil, output, n=None, stream=None):
+        _call("b2co_mset_contains_if", self._h, _ptr(keys), _ptr(stencil), _ptr(output),
+              C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def Find(self, keys, output, n=None, stream=None):
+        _call("b2co_mset_find", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def FindIf(self, keys, stencil, output, n=None, stream=None):
+        _call("b2co_mset_find_if", self._h, _ptr(keys), _ptr(stencil), _ptr(output),
+              C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def CountEach(self, keys, output, n=None, stream=None):
+        _call("b2co_mset_count_each", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def CountEachOuter(self, keys, output, n=None, stream=None):
+        _call("b2co_mset_count_each_outer", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def Count(self, keys, n=None, stream=None):
+        return self._u64("b2co_mset_count", _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def Retrieve(self, keys, probe_output, match_output, output_capacity, n=None, stream=None):
+        return self._u64("b2co_mset_retrieve", _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _ptr(probe_output),
+                         _ptr(match_output), C.c_uint64(output_capacity), _stream(stream))
+
+    def RetrieveAll(self, output, output_capacity, stream=None):
+        return self._u64("b2co_mset_retrieve_all", _ptr(output), C.c_uint64(output_capacity), _stream(stream))
+
+
+class StaticMultimap:
+    """StaticMultimap<Key, Value> (include/static_multimap.h), int32 / int64;
+    inputs are Pair<Key, Value> arrays (pack_pairs); synchronous."""
+
+    def __init__(self, capacity, empty_key, empty_value, key_dtype=None, value_dtype=None, stream=None):
+        import torch
+        self.key_bytes = _dtype_bytes(key_dtype or torch.int64)
+        self.value_bytes = _dtype_bytes(value_dtype or torch.int64)
+        h = C.c_void_p()
+        _call("b2co_mmap_create", C.c_uint64(capacity), C.c_uint32(self.key_bytes), C.c_uint32(self.value_bytes),
+              C.c_uint64(_bits(empty_key, self.key_bytes)), C.c_uint64(_bits(empty_value, self.value_bytes)),
+              _stream(stream), C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_mmap_destroy(h)
+            self._h = None
+
+    def _u64(self, name, *args):
+        v = C.c_uint64()
+        _call(name, self._h, *args, C.byref(v))
+        return v.value
+
+    def Capacity(self):
+        return self._u64("b2co_mmap_capacity")
+
+    def Size(self, stream=None):
+        return self._u64("b2co_mmap_size")
+
+    def Clear(self, stream=None):
+        _call("b2co_mmap_clear", self._h, _stream(stream))
+
+    def Insert(self, pairs, n=None, stream=None):
+        return self._u64("b2co_mmap_insert", _ptr(pairs), C.c_uint64(_OaBase._n(pairs, n)), _stream(stream))
+
+    def InsertIf(self, pairs, stencil, n=None, stream=None):
+        return self._u64("b2co_mmap_insert_if", _ptr(pairs), _ptr(stencil), C.c_uint64(_OaBase._n(pairs, n)),
+                         _stream(stream))
+
+    def Contains(self, keys, output, n=None, stream=None):
+        _call("b2co_mmap_contains", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def ContainsIf(self, keys, stencil, output, n=None, stream=None):
+        _call("b2co_mmap_contains_if", self._h, _ptr(keys), _ptr(stencil), _ptr(output),
+              C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def Find(self, keys, output, n=None, stream=None):
+        _call("b2co_mmap_find", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def FindIf(self, keys, stencil, output, n=None, stream=None):
+        _call("b2co_mmap_find_if", self._h, _ptr(keys), _ptr(stencil), _ptr(output),
+              C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def Count(self, keys, n=None, stream=None):
+        return self._u64("b2co_mmap_count", _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _stream(stream))
+
+    def Retrieve(self, keys, key_output, value_output, output_capacity, n=None, stream=None):
+        return self._u64("b2co_mmap_retrieve", _ptr(keys), C.c_uint64(_OaBase._n(keys, n)), _ptr(key_output),
+                         _ptr(value_output), C.c_uint64(output_capacity), _stream(stream))
+
+    def RetrieveAll(self, key_output, value_output, output_capacity, stream=None):
+        return self._u64("b2co_mmap_retrieve_all", _ptr(key_output), _ptr(value_output),
+                         C.c_uint64(output_capacity), _stream(stream))
 
 
 class BloomFilter:

@@ -157,6 +157,7 @@ const char* b2co_status_string(int s)
         case B2CO_ECUDA: return "CUDA runtime error";
         case B2CO_ETIMEOUT: return "device wait timed out";
         case B2CO_ELOGIC: return "logic error";
+        case B2CO_EOVERFLOW: return "overflow error";
     }
     return "unknown status";
 }
