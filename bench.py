@@ -517,6 +517,7 @@ def extra_measurements(t, keys, q50, out, stream, args):
     del q8
     res.update(bloom_hll_measurements(stream))
     res.update(batched_measurements(stream))
+    res.update(multi_measurements(stream))
     res.update(served_measurements(stream))
     return res
 
@@ -692,6 +693,80 @@ def bloom_part(f_time, g, peak):
 # ---------------------------------------------------------------------------
 # reference arm: the reference algorithm's CPU restatement on the host cores
 # ---------------------------------------------------------------------------
+
+def multi_measurements(stream, log2n=26):
+    """StaticMultimap<int64,int64> and StaticMultiset<int64>: 2^log2n entries
+    over 2^(log2n-2) distinct keys (uniform, about 4 per key); Insert, the lazy
+    grouped-index build of the multimap (first query after the insert), Find
+    and Count on 2^log2n queries at 50% hits, Retrieve on 2^(log2n-2) queries,
+    and the multiset's CountEach.  Device time by CUDA events on the stream
+    (the calls are synchronous, so host time is inside)."""
+    import torch
+    import b2co
+    n = 1 << log2n
+    lo = -(1 << 63)
+    g = torch.Generator(device="cuda").manual_seed(SEED + 21)
+    distinct = mix64_torch(counters(7 << 40, n >> 2, "torch")) >> 1  # halved: never the int64 sentinel
+    keys = distinct[torch.randint(0, n >> 2, (n,), generator=g, device="cuda")]
+    vals = mix64_torch(counters(8 << 40, n, "torch")) >> 1
+    q = torch.where(torch.rand(n, generator=g, device="cuda") < 0.5, distinct[torch.randint(0, n >> 2, (n,),
+                    generator=g, device="cuda")], mix64_torch(counters(9 << 40, n, "torch")) >> 1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    res = {"multi_entries": n, "multi_distinct_keys": n >> 2}
+    mm = b2co.StaticMultimap(n, lo, lo, key_dtype=torch.int64, value_dtype=torch.int64)
+    pairs = b2co.pack_pairs(keys, vals)
+    ms, failed = timed(lambda: mm.Insert(pairs))
+    assert failed == 0
+    res["multimap_insert_gpairs"] = round(n / ms / 1e6, 3)
+    ms, _ = timed(lambda: mm.Count(q[:1]))  # builds the grouped index
+    res["multimap_index_build_ms"] = round(ms, 2)
+    out = torch.empty(n, dtype=torch.int64, device="cuda")
+    mm.Find(q, out)
+    ms, _ = timed(lambda: mm.Find(q, out))
+    res["multimap_find_gkeys"] = round(n / ms / 1e6, 3)
+    ms, total = timed(lambda: mm.Count(q))
+    res["multimap_count_gkeys"] = round(n / ms / 1e6, 3)
+    qr = q[: n >> 2]
+    cnt = mm.Count(qr)
+    ko = torch.empty(cnt, dtype=torch.int64, device="cuda")
+    vo = torch.empty(cnt, dtype=torch.int64, device="cuda")
+    ms, w = timed(lambda: mm.Retrieve(qr, ko, vo, cnt))
+    assert w == cnt
+    res["multimap_retrieve_gkeys"] = round((n >> 2) / ms / 1e6, 3)
+    res["multimap_retrieve_gpairs_out"] = round(cnt / ms / 1e6, 3)
+    kk, vv = ko.cpu().numpy(), vo.cpu().numpy()
+    del mm, pairs, ko, vo, out
+    st = b2co.StaticMultiset(n, lo, key_dtype=torch.int64)
+    ms, failed = timed(lambda: st.Insert(keys))
+    assert failed == 0
+    res["multiset_insert_gkeys"] = round(n / ms / 1e6, 3)
+    ce = torch.empty(n, dtype=torch.int64, device="cuda")
+    st.CountEach(q, ce)
+    ms, _ = timed(lambda: st.CountEach(q, ce))
+    res["multiset_count_each_gkeys"] = round(n / ms / 1e6, 3)
+    res["multiset_count_matches_multimap"] = bool(int(ce.sum().item()) == total)
+    # size-independent checks of the multimap's Retrieve: each query's run has the
+    # multiset's multiplicity of its key and its values ascend within the run
+    per_query = ce[: n >> 2].cpu().numpy()
+    starts = np.zeros(len(vv), dtype=bool)
+    starts[np.cumsum(per_query)[:-1][per_query[1:] > 0]] = True
+    starts[0] = True
+    inner = ~starts[1:]
+    res["multimap_runs_ascending"] = bool(int(per_query.sum()) == len(vv) and (vv[1:][inner] >= vv[:-1][inner]).all()
+                                          and (kk[1:][inner] == kk[:-1][inner]).all())
+    del st, ce
+    torch.cuda.empty_cache()
+    return res
+
 
 SERVED_RATES = (1000, 2000, 5000, 10000, 20000, 50000, 200000)  # the last one is past saturation
 SERVED_STREAM, SERVED_MISS, SERVED_NEW, SERVED_VALUES = 3 << 40, 4 << 40, 5 << 40, 6 << 40
@@ -878,7 +953,7 @@ def main():
     ap.add_argument("--queries-log2", type=int, default=27, help="queries per step 2^k (profiling: smaller)")
     ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
-    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll", "hll"],
+    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll", "hll", "multi"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
     ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
     args = ap.parse_args()
@@ -889,7 +964,8 @@ def main():
     if args.only:
         import torch
         fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,
-              "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2)}[args.only]
+              "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2),
+              "multi": multi_measurements}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
         run_reference(args)

@@ -433,6 +433,217 @@ class DynamicMap {
     b2co_dmap* m_ = nullptr;
 };
 
+// ---- static_multiset.h -----------------------------------------------------
+template <class Key>
+class StaticMultiset {
+    static_assert(std::is_same<Key, int32_t>::value || std::is_same<Key, int64_t>::value,
+                  "StaticMultiset supports int32_t and int64_t keys");
+
+   public:
+    using Extent = b2co::Extent<std::size_t>;
+    using SizeType = std::size_t;
+    StaticMultiset(Extent capacity, Key emptyKey, cudaStream_t stream = nullptr)
+    {
+        throw_on(b2co_mset_create(static_cast<SizeType>(capacity), sizeof(Key), detail::bits_of(emptyKey),
+                                  to_stream(stream), &s_));
+    }
+    ~StaticMultiset() { b2co_mset_destroy(s_); }
+    StaticMultiset(StaticMultiset const&) = delete;
+    StaticMultiset& operator=(StaticMultiset const&) = delete;
+    StaticMultiset(StaticMultiset&& o) noexcept : s_{std::exchange(o.s_, nullptr)} {}
+    StaticMultiset& operator=(StaticMultiset&& o) noexcept
+    {
+        if (this != &o) {
+            b2co_mset_destroy(s_);
+            s_ = std::exchange(o.s_, nullptr);
+        }
+        return *this;
+    }
+    SizeType Capacity() const noexcept
+    {
+        uint64_t c = 0;
+        return b2co_mset_capacity(s_, &c) == B2CO_OK ? SizeType(c) : 0;
+    }
+    SizeType Size(cudaStream_t = nullptr) const { return get(b2co_mset_size); }
+    void Clear(cudaStream_t s = nullptr) { throw_on(b2co_mset_clear(s_, to_stream(s))); }
+    SizeType Insert(void* keys, Extent n, cudaStream_t s = nullptr)
+    {
+        uint64_t f = 0;
+        throw_on(b2co_mset_insert(s_, keys, static_cast<SizeType>(n), to_stream(s), &f));
+        return SizeType(f);
+    }
+    template <typename Stencil, typename Predicate = AlwaysTrue>
+    SizeType InsertIf(void* keys, Stencil* stencil, Extent n, cudaStream_t s = nullptr)
+    {
+        static_assert(sizeof(Stencil) == 1, "the C ABI carries uint8 stencils (nonzero = selected)");
+        uint64_t f = 0;
+        throw_on(b2co_mset_insert_if(s_, keys, reinterpret_cast<uint8_t const*>(stencil), static_cast<SizeType>(n),
+                                     to_stream(s), &f));
+        return SizeType(f);
+    }
+    void Contains(void* keys, void* out, Extent n, cudaStream_t s = nullptr)
+    {
+        throw_on(b2co_mset_contains(s_, keys, static_cast<uint8_t*>(out), static_cast<SizeType>(n), to_stream(s)));
+    }
+    void Contains(void* keys, Extent n, void* out, cudaStream_t s = nullptr) { Contains(keys, out, n, s); }
+    void Find(void* keys, void* out, Extent n, cudaStream_t s = nullptr)
+    {
+        throw_on(b2co_mset_find(s_, keys, out, static_cast<SizeType>(n), to_stream(s)));
+    }
+    void Find(void* keys, Extent n, void* out, cudaStream_t s = nullptr) { Find(keys, out, n, s); }
+    template <typename Stencil, typename Predicate = AlwaysTrue>
+    void ContainsIf(void* keys, Stencil* stencil, void* out, Extent n, cudaStream_t s = nullptr)
+    {
+        throw_on(b2co_mset_contains_if(s_, keys, reinterpret_cast<uint8_t const*>(stencil), static_cast<uint8_t*>(out),
+                                       static_cast<SizeType>(n), to_stream(s)));
+    }
+    template <typename Stencil, typename Predicate = AlwaysTrue>
+    void FindIf(void* keys, Stencil* stencil, void* out, Extent n, cudaStream_t s = nullptr)
+    {
+        throw_on(b2co_mset_find_if(s_, keys, reinterpret_cast<uint8_t const*>(stencil), out, static_cast<SizeType>(n),
+                                   to_stream(s)));
+    }
+    void CountEach(void* keys, void* out, Extent n, cudaStream_t s = nullptr)
+    {
+        throw_on(b2co_mset_count_each(s_, keys, static_cast<uint64_t*>(out), static_cast<SizeType>(n), to_stream(s)));
+    }
+    void CountEachOuter(void* keys, void* out, Extent n, cudaStream_t s = nullptr)
+    {
+        throw_on(b2co_mset_count_each_outer(s_, keys, static_cast<uint64_t*>(out), static_cast<SizeType>(n),
+                                            to_stream(s)));
+    }
+    SizeType Count(void* keys, Extent n, cudaStream_t s = nullptr)
+    {
+        uint64_t t = 0;
+        throw_on(b2co_mset_count(s_, keys, static_cast<SizeType>(n), to_stream(s), &t));
+        return SizeType(t);
+    }
+    SizeType Retrieve(void* keys, Extent n, void* probeOutput, void* matchOutput, Extent outputCapacity,
+                      cudaStream_t s = nullptr)
+    {
+        uint64_t w = 0;
+        throw_on(b2co_mset_retrieve(s_, keys, static_cast<SizeType>(n), probeOutput, matchOutput,
+                                    static_cast<SizeType>(outputCapacity), to_stream(s), &w));
+        return SizeType(w);
+    }
+    SizeType RetrieveAll(void* output, Extent outputCapacity, cudaStream_t s = nullptr)
+    {
+        uint64_t w = 0;
+        throw_on(b2co_mset_retrieve_all(s_, output, static_cast<SizeType>(outputCapacity), to_stream(s), &w));
+        return SizeType(w);
+    }
+
+   private:
+    template <class F>
+    SizeType get(F f) const
+    {
+        uint64_t v = 0;
+        throw_on(f(s_, &v));
+        return SizeType(v);
+    }
+    b2co_mset* s_ = nullptr;
+};
+
+// ---- static_multimap.h -----------------------------------------------------
+template <class Key, class Value>
+class StaticMultimap {
+    static_assert((std::is_same<Key, int32_t>::value || std::is_same<Key, int64_t>::value) &&
+                      (std::is_same<Value, int32_t>::value || std::is_same<Value, int64_t>::value),
+                  "StaticMultimap supports signed I32/I64 keys and values");
+
+   public:
+    using ExtentType = b2co::Extent<std::size_t>;
+    using SizeType = std::size_t;
+    StaticMultimap(ExtentType capacity, Key emptyKey, Value emptyValue, cudaStream_t stream = nullptr)
+    {
+        throw_on(b2co_mmap_create(static_cast<SizeType>(capacity), sizeof(Key), sizeof(Value),
+                                  detail::bits_of(emptyKey), detail::bits_of(emptyValue), to_stream(stream), &m_));
+    }
+    ~StaticMultimap() { b2co_mmap_destroy(m_); }
+    StaticMultimap(StaticMultimap const&) = delete;
+    StaticMultimap& operator=(StaticMultimap const&) = delete;
+    StaticMultimap(StaticMultimap&& o) noexcept : m_{std::exchange(o.m_, nullptr)} {}
+    StaticMultimap& operator=(StaticMultimap&& o) noexcept
+    {
+        if (this != &o) {
+            b2co_mmap_destroy(m_);
+            m_ = std::exchange(o.m_, nullptr);
+        }
+        return *this;
+    }
+    SizeType Capacity() const noexcept
+    {
+        uint64_t c = 0;
+        return b2co_mmap_capacity(m_, &c) == B2CO_OK ? SizeType(c) : 0;
+    }
+    SizeType Size(cudaStream_t = nullptr) const
+    {
+        uint64_t v = 0;
+        throw_on(b2co_mmap_size(m_, &v));
+        return SizeType(v);
+    }
+    void Clear(cudaStream_t s = nullptr) { throw_on(b2co_mmap_clear(m_, to_stream(s))); }
+    SizeType Insert(void* pairs, ExtentType n, cudaStream_t s = nullptr)
+    {
+        uint64_t f = 0;
+        throw_on(b2co_mmap_insert(m_, pairs, static_cast<SizeType>(n), to_stream(s), &f));
+        return SizeType(f);
+    }
+    template <class Stencil, class Predicate = AlwaysTrue>
+    SizeType InsertIf(void* pairs, Stencil* stencil, ExtentType n, cudaStream_t s = nullptr)
+    {
+        static_assert(sizeof(Stencil) == 1, "the C ABI carries uint8 stencils (nonzero = selected)");
+        uint64_t f = 0;
+        throw_on(b2co_mmap_insert_if(m_, pairs, reinterpret_cast<uint8_t const*>(stencil), static_cast<SizeType>(n),
+                                     to_stream(s), &f));
+        return SizeType(f);
+    }
+    void Contains(void* keys, void* output, ExtentType n, cudaStream_t s = nullptr) const
+    {
+        throw_on(b2co_mmap_contains(m_, keys, static_cast<uint8_t*>(output), static_cast<SizeType>(n), to_stream(s)));
+    }
+    template <class Stencil, class Predicate = AlwaysTrue>
+    void ContainsIf(void* keys, Stencil* stencil, void* output, ExtentType n, cudaStream_t s = nullptr) const
+    {
+        throw_on(b2co_mmap_contains_if(m_, keys, reinterpret_cast<uint8_t const*>(stencil),
+                                       static_cast<uint8_t*>(output), static_cast<SizeType>(n), to_stream(s)));
+    }
+    void Find(void* keys, void* output, ExtentType n, cudaStream_t s = nullptr) const
+    {
+        throw_on(b2co_mmap_find(m_, keys, output, static_cast<SizeType>(n), to_stream(s)));
+    }
+    template <class Stencil, class Predicate = AlwaysTrue>
+    void FindIf(void* keys, Stencil* stencil, void* output, ExtentType n, cudaStream_t s = nullptr) const
+    {
+        throw_on(b2co_mmap_find_if(m_, keys, reinterpret_cast<uint8_t const*>(stencil), output,
+                                   static_cast<SizeType>(n), to_stream(s)));
+    }
+    uint64_t Count(void* keys, ExtentType n, cudaStream_t s = nullptr) const
+    {
+        uint64_t t = 0;
+        throw_on(b2co_mmap_count(m_, keys, static_cast<SizeType>(n), to_stream(s), &t));
+        return t;
+    }
+    SizeType Retrieve(void* keys, ExtentType n, void* probeOut, void* valueOut, ExtentType outputCapacity,
+                      cudaStream_t s = nullptr) const
+    {
+        uint64_t w = 0;
+        throw_on(b2co_mmap_retrieve(m_, keys, static_cast<SizeType>(n), probeOut, valueOut,
+                                    static_cast<SizeType>(outputCapacity), to_stream(s), &w));
+        return SizeType(w);
+    }
+    SizeType RetrieveAll(void* keyOut, void* valueOut, ExtentType outputCapacity, cudaStream_t s = nullptr) const
+    {
+        uint64_t w = 0;
+        throw_on(b2co_mmap_retrieve_all(m_, keyOut, valueOut, static_cast<SizeType>(outputCapacity), to_stream(s),
+                                        &w));
+        return SizeType(w);
+    }
+
+   private:
+    b2co_mmap* m_ = nullptr;
+};
+
 // ---- bloom_filter.h --------------------------------------------------------
 // The reference's template parameters, in its order (bloom_filter_policy.h:42-48).
 // WordsPerBlock and PatternBits select the bits; the layout and

@@ -5,6 +5,7 @@
 // tests/test_cpp_api_gpu.py.
 #include <cstdio>
 #include <cstdlib>
+#include <limits>
 #include <random>
 #include <stdexcept>
 #include <unordered_map>
@@ -177,6 +178,36 @@ int main()
         using Seeded = b2co::BloomFilterPolicy<uint32_t, b2co::xxhash_64<uint32_t>, uint32_t, 8, 16, 1, 8, 1, 8, true, true>;
         b2co::BloomFilter<uint32_t, b2co::Extent<size_t>, Seeded> g(b2co::Extent<size_t>{257}, Seeded{b2co::xxhash_64<uint32_t>{42}}, stream);
         CHECK(g.NumWords() == 257 * 8);
+    }
+
+    // ---- StaticMultimap / StaticMultiset (contract_test.cpp:18-53, semantics_test.cpp) ----
+    {
+        using T = int64_t;
+        T const lo = std::numeric_limits<T>::lowest();
+        b2co::StaticMultimap<T, T> mm(b2co::Extent<size_t>{7}, lo, lo, stream);
+        std::vector<b2co::Pair<T, T>> pairs{{-7, 4}, {3, -8}, {3, -8}, {-7, -3}, {9, 7}, {3, 2}, {3, 9}};
+        DeviceBuffer<b2co::Pair<T, T>> dp(pairs);
+        CHECK(mm.Insert(dp.p, b2co::Extent<size_t>{pairs.size()}, stream) == 0);
+        DeviceBuffer<T> q(std::vector<T>{3, -7, 3, 42, lo});
+        DeviceBuffer<T> found(5);
+        mm.Find(q.p, found.p, b2co::Extent<size_t>{5}, stream);
+        CHECK((found.download() == std::vector<T>{-8, -3, -8, lo, lo}));
+        CHECK(mm.Count(q.p, b2co::Extent<size_t>{5}, stream) == 10);
+        DeviceBuffer<T> ok(10), ov(10);
+        CHECK(mm.Retrieve(q.p, b2co::Extent<size_t>{5}, ok.p, ov.p, b2co::Extent<size_t>{10}, stream) == 10);
+        CHECK((ov.download() == std::vector<T>{-8, -8, 2, 9, -3, 4, -8, -8, 2, 9}));
+        expect_throw<std::length_error>([&] { mm.Retrieve(q.p, b2co::Extent<size_t>{5}, ok.p, ov.p, b2co::Extent<size_t>{9}, stream); });
+        expect_throw<std::overflow_error>([&] { mm.Count(q.p, b2co::Extent<size_t>{std::numeric_limits<size_t>::max()}, stream); });
+        b2co::StaticMultiset<T> ms(b2co::Extent<size_t>{5}, lo, stream);
+        DeviceBuffer<T> keys(std::vector<T>{7, 2, 7, std::numeric_limits<T>::max(), -4, 2, 9});
+        CHECK(ms.Insert(keys.p, b2co::Extent<size_t>{7}, stream) == 2);
+        CHECK(ms.Size(stream) == 5);
+        DeviceBuffer<uint64_t> counts(7);
+        ms.CountEach(keys.p, counts.p, b2co::Extent<size_t>{7}, stream);
+        CHECK((counts.download() == std::vector<uint64_t>{2, 1, 2, 1, 1, 1, 0}));
+        auto moved = std::move(ms);
+        CHECK(moved.Size(stream) == 5);
+        expect_throw<std::logic_error>([&] { ms.Clear(stream); });
     }
 
     // ---- HyperLogLog<int64_t>: estimate within 3 standard errors ----
