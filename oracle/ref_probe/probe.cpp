@@ -12,6 +12,7 @@
 #include "extent.h"
 #include "bloom_filter_policy.h"
 #include "detail/hyperloglog/finalizer.h"
+#include "roaring_bitmap_ref.h"
 
 namespace {
 template <int B>
@@ -158,6 +159,34 @@ int ref_bloom_locate_policy(int key_bytes, uint64_t key, uint64_t num_blocks, ui
     B2CO_POLICY(32, 64)
 #undef B2CO_POLICY
     return -1;
+}
+
+// Roaring portable format: the reference's host parser (bounded by `bytes`),
+// then its membership query compiled for the host.  Returns 0, or 1 when the
+// parser rejects the input (the reference's std::invalid_argument).
+int ref_roaring(int key64, uint8_t const* data, uint64_t bytes, uint64_t const* keys, uint64_t n, uint8_t* out,
+                uint64_t* num_keys, uint64_t* size_bytes)
+{
+    try {
+        if (key64) {
+            auto parsed = aclco::detail::ParseRoaringBitmap<uint64_t>(data, bytes);
+            aclco::RoaringBitmapRef<uint64_t> ref(data, &parsed.metadata, parsed.buckets.data(),
+                                                  parsed.metadata.numKeys, parsed.metadata.sizeBytes);
+            for (uint64_t i = 0; i < n; ++i) out[i] = ref.Contains(keys[i]);
+            *num_keys = parsed.metadata.numKeys;
+            *size_bytes = parsed.metadata.sizeBytes;
+        } else {
+            auto parsed = aclco::detail::ParseRoaringBitmap<uint32_t>(data, bytes);
+            aclco::RoaringBitmapRef<uint32_t> ref(data, &parsed.metadata, parsed.metadata.numKeys,
+                                                  parsed.metadata.sizeBytes);
+            for (uint64_t i = 0; i < n; ++i) out[i] = ref.Contains(static_cast<uint32_t>(keys[i]));
+            *num_keys = parsed.metadata.numKeys;
+            *size_bytes = parsed.metadata.sizeBytes;
+        }
+    } catch (std::invalid_argument const&) {
+        return 1;
+    }
+    return 0;
 }
 
 uint64_t ref_hll_finalize(int precision, double z, int v)

@@ -38,6 +38,7 @@ def load_probe(ref: str):
         "ref_probe_walk": (None, [i32, i32, i32, i32, u64, u32, u32, C.c_void_p]),
         "ref_bloom_locate": (None, [i32, u64, u64, u64, C.c_void_p, C.c_void_p]),
         "ref_bloom_locate_policy": (i32, [i32, u64, u64, u64, u32, u32, C.c_void_p, C.c_void_p]),
+        "ref_roaring": (i32, [i32, C.c_void_p, u64, C.c_void_p, u64, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ref_hll_finalize": (u64, [i32, dbl, i32]),
         "ref_hll_points": (i32, [i32]), "ref_hll_raw": (dbl, [i32, i32]),
         "ref_hll_bias": (dbl, [i32, i32]), "ref_hll_threshold": (dbl, [i32]),
@@ -191,6 +192,26 @@ def hll(L, rng):
     return {"tables": tables, "finalizer_cases": cases}
 
 
+def roaring(L, rng):
+    """The reference's own portable-format parser and membership query
+    (roaring_bitmap_ref.h, detail/roaring_bitmap/format.h) over the oracle's
+    deterministic cases: validity, key count, serialized size, Contains."""
+    from oracle.roaring import golden_cases
+    rows = []
+    for name, key64, _, data, queries, valid in golden_cases():
+        q = np.ascontiguousarray(queries, dtype=np.uint64)
+        out = np.zeros(len(q), dtype=np.uint8)
+        nk, sb = C.c_uint64(), C.c_uint64()
+        buf = C.create_string_buffer(data, len(data))
+        st = L.ref_roaring(int(key64), buf, len(data), q.ctypes.data, len(q), out.ctypes.data, C.byref(nk),
+                           C.byref(sb))
+        assert (st == 0) == valid, name
+        rows.append({"name": name, "key64": bool(key64), "hex": data.hex(), "valid": st == 0,
+                     "num_keys": nk.value if st == 0 else None, "size_bytes": sb.value if st == 0 else None,
+                     "queries": [int(x) for x in q], "contains": out.tolist() if st == 0 else None})
+    return {"bitmaps": rows}
+
+
 def main():
     import sys
     sys.path.insert(0, REPO)
@@ -200,7 +221,7 @@ def main():
     L = load_probe(args.ref)
     rng = np.random.default_rng(2026)
     for name, fn in [("hashes", hashes), ("capacity", capacity), ("probing", probing), ("bloom", bloom),
-                     ("hll", hll)]:
+                     ("hll", hll), ("roaring", roaring)]:
         data = fn(L, rng)
         with open(os.path.join(HERE, f"{name}.json"), "w") as f:
             json.dump(data, f, separators=(",", ":"))

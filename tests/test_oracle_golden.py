@@ -183,3 +183,21 @@ def test_oracle_hll_registers_rule():
             ref[idx] = max(ref[idx], rank)
         assert (reg == ref).all()
         assert reg.max() <= 65 - p
+
+
+def test_roaring_oracle_matches_reference():
+    """The Roaring oracle (oracle/roaring.py) against the reference's own parser
+    and membership query (roaring_bitmap_ref.h, detail/roaring_bitmap/format.h,
+    compiled on the host by tests/golden/make_golden.py): the serializer
+    reproduces the recorded bytes and the set-based Contains equals the
+    reference's answers on every query."""
+    from oracle.roaring import contains, golden_cases
+    rows = {r["name"]: r for r in load("roaring")["bitmaps"]}
+    for name, key64, elements, data, queries, valid in golden_cases():
+        r = rows[name]
+        assert r["hex"] == data.hex(), name
+        assert r["valid"] == valid and r["key64"] == key64, name
+        assert r["queries"] == [int(x) for x in queries], name
+        if valid:
+            assert r["num_keys"] == len(np.unique(elements)) and r["size_bytes"] == len(data), name
+            assert contains(elements, queries).astype(int).tolist() == r["contains"], name
