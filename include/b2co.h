@@ -399,6 +399,33 @@ int b2co_mmap_retrieve_all(b2co_mmap* map, void* key_out, void* value_out, uint6
                            b2co_stream stream, uint64_t* written);
 
 /* ===================================================================== */
+/* RoaringBitmap<Key>, Key uint32 or uint64, portable serialization         */
+/* ===================================================================== */
+typedef struct b2co_roaring b2co_roaring;
+/* reference: include/roaring_bitmap.h:49-77 constructors, parse rules of
+ * detail/roaring_bitmap/format.h:164-318: the serialized bitmap (cookie
+ * 12346 / 12347 32-bit form, or the 64-bit bucketed form for key_bytes 8) is
+ * parsed and validated on the host, then copied to the device.
+ * available_bytes bounds the parse (UINT64_MAX: the input is trusted, as in
+ * the reference's unbounded constructor); malformed or truncated input ->
+ * EINVAL, as the reference's std::invalid_argument. */
+int b2co_roaring_create(const void* host_bytes, uint64_t available_bytes, uint32_t key_bytes, b2co_stream stream,
+                        b2co_roaring** out);
+int b2co_roaring_destroy(b2co_roaring* bitmap);
+/* Host only: the validation and measurement the constructor runs. */
+int b2co_roaring_parse(const void* host_bytes, uint64_t available_bytes, uint32_t key_bytes, uint64_t* num_keys,
+                       uint64_t* size_bytes);
+/* reference: roaring_bitmap.h:88-108 Contains / ContainsAsync: out[i] (1 byte)
+ * = keys[i] is in the bitmap; NULL buffers only with n == 0. */
+int b2co_roaring_contains(b2co_roaring* bitmap, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+int b2co_roaring_contains_async(b2co_roaring* bitmap, const void* keys, uint8_t* out, uint64_t n, b2co_stream stream);
+/* reference: roaring_bitmap.h:110-118 Size (keys), SizeBytes, Data (device copy
+ * of the serialized bytes); Empty() is Size() == 0. */
+int b2co_roaring_size(const b2co_roaring* bitmap, uint64_t* num_keys);
+int b2co_roaring_size_bytes(const b2co_roaring* bitmap, uint64_t* size_bytes);
+int b2co_roaring_data(const b2co_roaring* bitmap, const uint8_t** device_bytes);
+
+/* ===================================================================== */
 /* BloomFilter<Key>, default policy (8 x uint32 words per block, xxh64)     */
 /* ===================================================================== */
 

@@ -776,6 +776,66 @@ class StaticMultimap:
                          C.c_uint64(output_capacity), _stream(stream))
 
 
+def roaring_parse(data: bytes, key_bytes: int = 4, bounded: bool = True):
+    """(num_keys, size_bytes) of a serialized portable Roaring bitmap (host
+    only; the validation RoaringBitmap's constructor runs)."""
+    nk, sb = C.c_uint64(), C.c_uint64()
+    buf = C.create_string_buffer(bytes(data), len(data))
+    _call("b2co_roaring_parse", buf, C.c_uint64(len(data) if bounded else 2**64 - 1), C.c_uint32(key_bytes),
+          C.byref(nk), C.byref(sb))
+    return nk.value, sb.value
+
+
+class RoaringBitmap:
+    """RoaringBitmap<Key> (include/roaring_bitmap.h) over a portable
+    serialized bitmap held in host memory; Key uint32 (key_bytes 4) or uint64
+    (key_bytes 8, the 64-bit bucketed form)."""
+
+    def __init__(self, data: bytes, key_bytes: int = 4, bounded: bool = True, stream=None):
+        self.key_bytes = key_bytes
+        h = C.c_void_p()
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _call("b2co_roaring_create", buf, C.c_uint64(len(data) if bounded else 2**64 - 1), C.c_uint32(key_bytes),
+              _stream(stream), C.byref(h))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.b2co_roaring_destroy(h)
+            self._h = None
+
+    def Contains(self, keys, output, n=None, stream=None):
+        _call("b2co_roaring_contains", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def ContainsAsync(self, keys, output, n=None, stream=None):
+        _call("b2co_roaring_contains_async", self._h, _ptr(keys), _ptr(output), C.c_uint64(_OaBase._n(keys, n)),
+              _stream(stream))
+
+    def Size(self) -> int:
+        v = C.c_uint64()
+        _call("b2co_roaring_size", self._h, C.byref(v))
+        return v.value
+
+    def Empty(self) -> bool:
+        return self.Size() == 0
+
+    def SizeBytes(self) -> int:
+        v = C.c_uint64()
+        _call("b2co_roaring_size_bytes", self._h, C.byref(v))
+        return v.value
+
+    def Data(self) -> int:
+        p = C.c_void_p()
+        _call("b2co_roaring_data", self._h, C.byref(p))
+        return p.value
+
+    def bytes(self) -> bytes:
+        """The device copy of the serialized bitmap, read back."""
+        return _device_bytes(self.Data(), self.SizeBytes()).tobytes()
+
+
 class BloomFilter:
     """BloomFilter<Key, Extent, BloomFilterPolicy<Key, xxhash_64<Key>, uint32_t,
     WordsPerBlock, PatternBits>> (include/bloom_filter.h:37-39,
