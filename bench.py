@@ -518,6 +518,7 @@ def extra_measurements(t, keys, q50, out, stream, args):
     res.update(bloom_hll_measurements(stream))
     res.update(batched_measurements(stream))
     res.update(multi_measurements(stream))
+    res.update(roaring_measurements(stream))
     res.update(served_measurements(stream))
     return res
 
@@ -768,6 +769,66 @@ def multi_measurements(stream, log2n=26):
     return res
 
 
+def roaring_serialize32(values: np.ndarray) -> bytes:
+    """Portable Roaring serialization (cookie 12346: arrays and bitsets, with
+    offsets) of a set of uint32 values -- the bench's own input builder."""
+    import struct
+    vals = np.unique(values.astype(np.uint32))
+    hi = (vals >> 16).astype(np.uint32)
+    keys, starts = np.unique(hi, return_index=True)
+    bounds = np.append(starts, len(vals))
+    bodies = []
+    for i in range(len(keys)):
+        lo = (vals[bounds[i]:bounds[i + 1]] & 0xFFFF).astype(np.uint16)
+        if len(lo) <= 4096:
+            bodies.append((len(lo), lo.astype("<u2").tobytes()))
+        else:
+            bits = np.zeros(65536, dtype=np.uint8)
+            bits[lo] = 1
+            bodies.append((len(lo), np.packbits(bits, bitorder="little").tobytes()))
+    n = len(keys)
+    head = bytearray(struct.pack("<II", 12346, n))
+    head += np.stack([keys.astype(np.uint16), np.array([c - 1 for c, _ in bodies], np.uint16)], 1).astype("<u2").tobytes()
+    pos = len(head) + 4 * n
+    offs = np.cumsum([pos] + [len(b) for _, b in bodies[:-1]]).astype("<u4") if n else np.zeros(0, "<u4")
+    return bytes(head) + offs.tobytes() + b"".join(b for _, b in bodies)
+
+
+def roaring_measurements(stream, log2q=27):
+    """RoaringBitmap<uint32_t> Contains on 2^log2q queries at 50% hits against
+    (a) a sparse bitmap: 2^24 uniform keys over the whole 32-bit range (65,536
+    array containers of ~256) and (b) a dense one: 2^26 even keys in 2,048
+    bitset containers.  Device time by CUDA events on the stream."""
+    import torch
+    import b2co
+    res = {}
+    rng = np.random.default_rng(SEED + 31)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nq = 1 << log2q
+    for name, vals in [("sparse", rng.integers(0, 2**32, size=1 << 24, dtype=np.uint64)),
+                       ("dense", np.arange(1 << 26, dtype=np.uint64) * 2)]:
+        data = roaring_serialize32(vals)
+        bm = b2co.RoaringBitmap(data, 4)
+        u = np.unique(vals.astype(np.uint32))
+        hits = u[rng.integers(0, len(u), size=nq // 2)]
+        q = np.concatenate([hits, rng.integers(0, 2**32, size=nq - nq // 2, dtype=np.uint64).astype(np.uint32)])
+        rng.shuffle(q)
+        qd = torch.from_numpy(q.view(np.int32)).cuda()
+        out = torch.empty(nq, dtype=torch.uint8, device="cuda")
+        bm.ContainsAsync(qd, out)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(5):
+            bm.ContainsAsync(qd, out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[f"roaring_{name}_contains_gkeys"] = round(5 * nq / e0.elapsed_time(e1) / 1e6, 3)
+        res[f"roaring_{name}_bitmap_bytes"] = bm.SizeBytes()
+        res[f"roaring_{name}_hits_found"] = bool(int(out.sum().item()) >= nq // 2)  # every planted hit at least
+        del bm, qd, out
+    return res
+
+
 SERVED_RATES = (1000, 2000, 5000, 10000, 20000, 50000, 200000)  # the last one is past saturation
 SERVED_STREAM, SERVED_MISS, SERVED_NEW, SERVED_VALUES = 3 << 40, 4 << 40, 5 << 40, 6 << 40
 
@@ -953,7 +1014,7 @@ def main():
     ap.add_argument("--queries-log2", type=int, default=27, help="queries per step 2^k (profiling: smaller)")
     ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
-    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll", "hll", "multi"],
+    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
     ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
     args = ap.parse_args()
@@ -965,7 +1026,7 @@ def main():
         import torch
         fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,
               "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2),
-              "multi": multi_measurements}[args.only]
+              "multi": multi_measurements, "roaring": roaring_measurements}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
         run_reference(args)

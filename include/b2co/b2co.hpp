@@ -644,6 +644,65 @@ class StaticMultimap {
     b2co_mmap* m_ = nullptr;
 };
 
+// ---- roaring_bitmap.h ------------------------------------------------------
+template <typename Key, typename ExtentT = Extent<std::size_t>>
+class RoaringBitmap {
+    static_assert(std::is_same<Key, uint32_t>::value || std::is_same<Key, uint64_t>::value,
+                  "RoaringBitmap key type must be uint32_t or uint64_t");
+
+   public:
+    using KeyType = Key;
+    using SizeType = typename ExtentT::ValueType;
+    // A complete, trusted serialized bitmap in host memory (length from the format).
+    explicit RoaringBitmap(void const* bitmap, cudaStream_t stream = nullptr) : RoaringBitmap(bitmap, ~std::size_t(0), stream) {}
+    // A serialized bitmap of at most bitmapBytes bytes; the parse is bounds-checked.
+    RoaringBitmap(void const* bitmap, std::size_t bitmapBytes, cudaStream_t stream = nullptr)
+    {
+        throw_on(b2co_roaring_create(bitmap, bitmapBytes, sizeof(Key), to_stream(stream), &r_));
+    }
+    ~RoaringBitmap() { b2co_roaring_destroy(r_); }
+    RoaringBitmap(RoaringBitmap const&) = delete;
+    RoaringBitmap& operator=(RoaringBitmap const&) = delete;
+    RoaringBitmap(RoaringBitmap&& o) noexcept : r_{std::exchange(o.r_, nullptr)} {}
+    RoaringBitmap& operator=(RoaringBitmap&& o) noexcept
+    {
+        if (this != &o) {
+            b2co_roaring_destroy(r_);
+            r_ = std::exchange(o.r_, nullptr);
+        }
+        return *this;
+    }
+    void Contains(void const* keys, void* outputValues, ExtentT keyNum, cudaStream_t stream) const
+    {
+        throw_on(b2co_roaring_contains(r_, keys, static_cast<uint8_t*>(outputValues), static_cast<SizeType>(keyNum),
+                                       to_stream(stream)));
+    }
+    void ContainsAsync(void const* keys, void* outputValues, ExtentT keyNum, cudaStream_t stream) const
+    {
+        throw_on(b2co_roaring_contains_async(r_, keys, static_cast<uint8_t*>(outputValues),
+                                             static_cast<SizeType>(keyNum), to_stream(stream)));
+    }
+    uint64_t Size() const noexcept
+    {
+        uint64_t v = 0;
+        return b2co_roaring_size(r_, &v) == B2CO_OK ? v : 0;
+    }
+    bool Empty() const noexcept { return Size() == 0; }
+    uint64_t SizeBytes() const noexcept
+    {
+        uint64_t v = 0;
+        return b2co_roaring_size_bytes(r_, &v) == B2CO_OK ? v : 0;
+    }
+    uint8_t const* Data() const noexcept
+    {
+        uint8_t const* p = nullptr;
+        return b2co_roaring_data(r_, &p) == B2CO_OK ? p : nullptr;
+    }
+
+   private:
+    b2co_roaring* r_ = nullptr;
+};
+
 // ---- bloom_filter.h --------------------------------------------------------
 // The reference's template parameters, in its order (bloom_filter_policy.h:42-48).
 // WordsPerBlock and PatternBits select the bits; the layout and

@@ -5,14 +5,16 @@
 // verbatim in device memory (Data()), and queried with Contains.
 //
 // B200 design: the host parse also flattens the container directory -- every
-// container's high key (u16, binary-searched), kind, cardinality and byte
-// offset, and for 64-bit keys every bucket's high key and container range --
-// into small device arrays.  A query block loads the key directories into
-// shared memory when they fit, so a lookup is a binary search over on-chip
-// keys followed by one container probe in the serialized bytes: an array
-// (binary search of sorted u16), a bitset (one byte) or a run container
-// (binary search of run starts).  Container data sit at arbitrary byte
-// offsets, so 16-bit fields are read byte-wise.
+// container's high key (u16), kind, cardinality and byte offset, and for
+// 64-bit keys every bucket's high key and container range -- into small device
+// arrays.  For 32-bit keys a direct table maps each of the 65,536 high keys to
+// its container (256 KiB, L2-resident), so a lookup is one table read plus one
+// container probe; for 64-bit keys a query block stages the bucket and
+// container keys in shared memory when they fit and binary-searches them.  The
+// container probe reads the serialized bytes: an array (binary search of
+// sorted u16), a bitset (one byte) or a run container (binary search of run
+// starts).  Container data may sit at odd byte offsets; such containers are
+// read byte-wise, the others with 16-bit loads.
 #include <algorithm>
 #include <limits>
 #include <new>
@@ -31,7 +33,8 @@ constexpr uint32_t kMaxArray = 4096;
 constexpr uint32_t kBitsetBytes = 8192;
 constexpr uint32_t kNoOffsetThreshold = 4;
 
-enum : uint32_t { kArray = 0, kBitset = 1, kRun = 2 };
+enum : uint32_t { kArray = 0, kBitset = 1, kRun = 2, kKindMask = 0xff, kAligned = 0x100 };
+constexpr uint32_t kNoContainer = 0xffffffffu;
 
 struct alignas(16) Container {
     unsigned long long offset;  // bytes from the start of the serialized data
@@ -121,6 +124,7 @@ int parse32(uint8_t const* data, uint64_t avail, uint64_t base, std::vector<uint
             kind = kBitset;
         }
         if (!r.require(off, bytes) || !r.ok) return fail(B2CO_EINVAL, "RoaringBitmap: truncated serialized bitmap");
+        if (((base + off) & 1) == 0) kind |= kAligned;  // 16-bit fields can be loaded as u16
         out.push_back(Container{base + off, card, kind});
         prev_end = off + bytes;
     }
@@ -190,12 +194,15 @@ __device__ __forceinline__ uint32_t lower_bound(T const* keys, uint32_t lo, uint
 __device__ __forceinline__ bool container_has(uint8_t const* bytes, Container const& c, uint32_t low)
 {
     uint8_t const* p = bytes + c.offset;
-    if (c.kind == kBitset) return (__ldg(p + (low >> 3)) >> (low & 7)) & 1u;
-    if (c.kind == kArray) {
+    uint32_t const kind = c.kind & kKindMask;
+    if (kind == kBitset) return (__ldg(p + (low >> 3)) >> (low & 7)) & 1u;
+    if (kind == kArray) {
         uint32_t lo = 0, hi = c.card;
+        uint16_t const* a = reinterpret_cast<uint16_t const*>(p);
+        bool const aligned = c.kind & kAligned;
         while (lo < hi) {
             uint32_t const mid = (lo + hi) >> 1;
-            uint32_t const v = ld16(p + 2 * mid);
+            uint32_t const v = aligned ? uint32_t(__ldg(a + mid)) : ld16(p + 2 * mid);
             if (v == low) return true;
             if (v < low) lo = mid + 1;
             else hi = mid;
@@ -218,39 +225,43 @@ __device__ __forceinline__ bool container_has(uint8_t const* bytes, Container co
 constexpr uint32_t kSharedKeys = 16384;  // u16 container keys staged per block (32 KiB)
 constexpr uint32_t kSharedBuckets = 2048;
 
-template <int KB>
-__global__ void __launch_bounds__(256) k_roaring_contains(uint8_t const* bytes, uint16_t const* ckeys,
-                                                          Container const* cont, uint32_t ncont,
-                                                          uint32_t const* bkeys, uint32_t const* bstart,
-                                                          uint32_t nbuckets, void const* keys, uint8_t* out,
-                                                          uint64_t n, bool stage)
+// 32-bit keys: a direct table from the 16-bit high key to the container
+// (65,536 entries, 256 KiB, L2-resident) replaces the directory search.
+__global__ void __launch_bounds__(256) k_roaring_contains32(uint8_t const* bytes, uint32_t const* direct,
+                                                            Container const* cont, uint32_t const* keys, uint8_t* out,
+                                                            uint64_t n)
+{
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        uint32_t const key = __ldg(keys + i);
+        uint32_t const c = __ldg(direct + (key >> 16));
+        out[i] = c != kNoContainer && container_has(bytes, cont[c], key & 0xffffu);
+    }
+}
+
+// 64-bit keys: bucket search, then the bucket's container directory, both on
+// chip when they fit.
+__global__ void __launch_bounds__(256) k_roaring_contains64(uint8_t const* bytes, uint16_t const* ckeys,
+                                                            Container const* cont, uint32_t ncont,
+                                                            uint32_t const* bkeys, uint32_t const* bstart,
+                                                            uint32_t nbuckets, unsigned long long const* keys,
+                                                            uint8_t* out, uint64_t n, bool stage)
 {
     __shared__ uint16_t s_ckeys[kSharedKeys];
     __shared__ uint32_t s_bkeys[kSharedBuckets];
     if (stage) {
         for (uint32_t i = threadIdx.x; i < ncont; i += blockDim.x) s_ckeys[i] = ckeys[i];
-        if (KB == 8)
-            for (uint32_t i = threadIdx.x; i < nbuckets; i += blockDim.x) s_bkeys[i] = bkeys[i];
+        for (uint32_t i = threadIdx.x; i < nbuckets; i += blockDim.x) s_bkeys[i] = bkeys[i];
         __syncthreads();
     }
     uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        uint64_t key;
-        if constexpr (KB == 8) key = __ldg(static_cast<unsigned long long const*>(keys) + i);
-        else key = __ldg(static_cast<uint32_t const*>(keys) + i);
-        uint32_t lo = 0, hi = ncont;
-        bool found = true;
-        if constexpr (KB == 8) {
-            uint32_t const hk = uint32_t(key >> 32);
-            uint32_t const b = stage ? lower_bound(s_bkeys, 0, nbuckets, hk) : lower_bound(bkeys, 0, nbuckets, hk);
-            found = b < nbuckets && (stage ? s_bkeys[b] : bkeys[b]) == hk;
-            if (found) {
-                lo = bstart[b];
-                hi = bstart[b + 1];
-            }
-        }
+        uint64_t const key = __ldg(keys + i);
+        uint32_t const hk = uint32_t(key >> 32);
+        uint32_t const b = stage ? lower_bound(s_bkeys, 0, nbuckets, hk) : lower_bound(bkeys, 0, nbuckets, hk);
         uint8_t r = 0;
-        if (found && lo < hi) {
+        if (b < nbuckets && (stage ? s_bkeys[b] : bkeys[b]) == hk) {
+            uint32_t const lo = bstart[b], hi = bstart[b + 1];
             uint32_t const ck = uint32_t(key >> 16) & 0xffffu;
             uint32_t const c = stage ? lower_bound(s_ckeys, lo, hi, ck) : lower_bound(ckeys, lo, hi, ck);
             if (c < hi && (stage ? uint32_t(s_ckeys[c]) : uint32_t(ckeys[c])) == ck)
@@ -272,6 +283,7 @@ struct b2co_roaring {
     Container* cont = nullptr;
     uint32_t* bkeys = nullptr;
     uint32_t* bstart = nullptr;
+    uint32_t* direct = nullptr;  // 32-bit keys: high key -> container
     uint32_t ncont = 0, nbuckets = 0;
 };
 
@@ -298,10 +310,18 @@ int contains_impl(b2co_roaring* r, void const* keys, uint8_t* out, uint64_t n, c
     if (n == 0) return B2CO_OK;
     if (!keys || !out) return fail(B2CO_EINVAL, "RoaringBitmap: null input or output with a nonzero key count");
     if (n > kMaxBatch) return fail(B2CO_ERANGE, "RoaringBitmap: batch exceeds the 32-bit index range");
-    bool const stage = r->ncont <= kSharedKeys && r->nbuckets <= kSharedBuckets;
-    auto k = r->key_bytes == 8 ? k_roaring_contains<8> : k_roaring_contains<4>;
-    k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(r->bytes, r->ckeys, r->cont, r->ncont, r->bkeys,
-                                                           r->bstart, r->nbuckets, keys, out, n, stage);
+    if (r->key_bytes == 4) {
+        auto k = k_roaring_contains32;
+        k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(r->bytes, r->direct, r->cont,
+                                                               static_cast<uint32_t const*>(keys), out, n);
+    } else {
+        bool const stage = r->ncont <= kSharedKeys && r->nbuckets <= kSharedBuckets;
+        auto k = k_roaring_contains64;
+        k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(r->bytes, r->ckeys, r->cont, r->ncont, r->bkeys,
+                                                               r->bstart, r->nbuckets,
+                                                               static_cast<unsigned long long const*>(keys), out, n,
+                                                               stage);
+    }
     B2CO_CUDA(cudaGetLastError());
     return B2CO_OK;
 }
@@ -344,6 +364,12 @@ int b2co_roaring_create(void const* host_bytes, uint64_t available_bytes, uint32
     if (!st) st = upload(&r->cont, p.cont, s);
     if (!st) st = upload(&r->bkeys, p.bkeys, s);
     if (!st) st = upload(&r->bstart, p.bstart.empty() ? std::vector<uint32_t>{0u} : p.bstart, s);
+    if (!st && key_bytes == 4) {
+        std::vector<uint32_t> direct(1u << 16, kNoContainer);
+        for (uint32_t c = 0; c < r->ncont; ++c) direct[p.ckeys[c]] = c;
+        st = upload(&r->direct, direct, s);
+        if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = cuda_fail(cudaGetLastError(), "RoaringBitmap upload");
+    }
     if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = cuda_fail(cudaGetLastError(), "RoaringBitmap upload");
     if (st) {
         b2co_roaring_destroy(r);
@@ -361,6 +387,7 @@ int b2co_roaring_destroy(b2co_roaring* r)
     cudaFree(r->cont);
     cudaFree(r->bkeys);
     cudaFree(r->bstart);
+    cudaFree(r->direct);
     delete r;
     return B2CO_OK;
 }

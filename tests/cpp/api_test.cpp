@@ -210,6 +210,20 @@ int main()
         expect_throw<std::logic_error>([&] { ms.Clear(stream); });
     }
 
+    // ---- RoaringBitmap<uint32_t>: the three-key portable bitmap (roaring_bitmap_factory.h AcceptanceKeys) ----
+    {
+        // cookie 12346, one container: key 1, cardinality 3 (stored as 2), offset 16, values 2, 4, 8
+        std::vector<uint8_t> bytes{0x3a, 0x30, 0, 0, 1, 0, 0, 0, 1, 0, 2, 0, 16, 0, 0, 0, 2, 0, 4, 0, 8, 0};
+        b2co::RoaringBitmap<uint32_t> rb(bytes.data(), bytes.size(), stream);
+        CHECK(rb.Size() == 3 && rb.SizeBytes() == bytes.size() && !rb.Empty());
+        DeviceBuffer<uint32_t> q(std::vector<uint32_t>{(1u << 16) | 2u, (1u << 16) | 3u, (1u << 16) | 8u, 2u});
+        DeviceBuffer<uint8_t> out(4);
+        rb.Contains(q.p, out.p, b2co::Extent<size_t>{4}, stream);
+        CHECK((out.download() == std::vector<uint8_t>{1, 0, 1, 0}));
+        std::vector<uint8_t> truncated(bytes.begin(), bytes.end() - 2);
+        expect_throw<std::invalid_argument>([&] { b2co::RoaringBitmap<uint32_t> bad(truncated.data(), truncated.size(), stream); });
+    }
+
     // ---- HyperLogLog<int64_t>: estimate within 3 standard errors ----
     {
         auto h = b2co::HyperLogLog<int64_t>::CreateWithSketchSizeKB(64, stream);
