@@ -311,7 +311,9 @@ def run_gpu(args):
         b2co.set_l2_fetch_granularity(args.l2_fetch)
     if args.sweep:
         sweep = {}
-        for shape in ["2x2", "2x2w", "2x1w", "4x1w", "4x2w", "4x4w", "8x4w", "4x2", "2x2s"]:
+        shapes = args.sweep_shapes.split(",") if args.sweep_shapes else [
+            "2x2", "2x2w", "2x1w", "4x1w", "4x2w", "4x4w", "8x4w", "4x2", "2x2s"]
+        for shape in shapes:
             t.set_find_shape(*parse_shape(shape))
             for _ in range(3):
                 t.FindAsync(q, out)
@@ -1013,6 +1015,7 @@ def main():
     ap.add_argument("--capacity-log2", type=int, default=28, help="requested capacity 2^k (profiling: smaller)")
     ap.add_argument("--queries-log2", type=int, default=27, help="queries per step 2^k (profiling: smaller)")
     ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
+    ap.add_argument("--sweep-shapes", default="", help="comma-separated shapes for --sweep (default: a fixed list)")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
     ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")

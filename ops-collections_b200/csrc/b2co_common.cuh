@@ -31,13 +31,27 @@ __device__ __forceinline__ unsigned long long cas_slot(unsigned long long* p, un
 }
 __device__ __forceinline__ U128 cas_slot(U128* p, U128 e, U128 d) { return atomicCAS(p, e, d); }
 
-// Read-only (non-coherent) loads for kernels that never write the table.
-__device__ __forceinline__ uint32_t ld_ro(uint32_t const* p) { return __ldg(p); }
-__device__ __forceinline__ unsigned long long ld_ro(unsigned long long const* p) { return __ldg(p); }
+// Read-only (non-coherent) loads for kernels that never write the table, with
+// the 64-byte L2 prefetch-size hint: a bucket window is a random 80-byte read,
+// and larger fills only bring in neighbouring slots no query of this launch is
+// likely to touch.
+__device__ __forceinline__ uint32_t ld_ro(uint32_t const* p)
+{
+    uint32_t v;
+    asm("ld.global.nc.L2::64B.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ unsigned long long ld_ro(unsigned long long const* p)
+{
+    unsigned long long v;
+    asm("ld.global.nc.L2::64B.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
 __device__ __forceinline__ U128 ld_ro(U128 const* p)
 {
-    ulonglong2 v = __ldg(reinterpret_cast<ulonglong2 const*>(p));
-    return U128{v.x, v.y};
+    unsigned long long lo, hi;
+    asm("ld.global.nc.L2::64B.v2.u64 {%0, %1}, [%2];" : "=l"(lo), "=l"(hi) : "l"(p));
+    return U128{lo, hi};
 }
 // ---- bulk copies (TMA, untiled) and mbarriers --------------------------------
 __device__ __forceinline__ uint32_t smem_u32(void const* p) { return uint32_t(__cvta_generic_to_shared(p)); }

@@ -68,15 +68,18 @@ int check_batch(uint64_t n)
 
 cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 
-// Default lookup shape per layout; the autotuner overrides it per table.
+// Default lookup shape per layout; b2co_oa_set_find_shape overrides it per table.
 void default_shape(b2co_oa_table* t)
 {
     if (t->desc.bucket_size == 1) {
         t->find_lanes = 1;  // a one-slot window needs no cooperation
         t->find_items = 4;
     } else {
-        t->find_lanes = 2;  // staged keys, two lanes per bucket window, two windows in flight per pair
-        t->find_items = 2;
+        // keys staged per warp (no block barrier: a warp whose keys need further
+        // windows holds up no other warp), two lanes per bucket window, two
+        // windows in flight per pair
+        t->find_lanes = 2;
+        t->find_items = 2 | kShapeWarpStaged;
     }
 }
 

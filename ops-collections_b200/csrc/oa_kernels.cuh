@@ -168,7 +168,7 @@ __device__ __forceinline__ void warp_add_counter(unsigned long long* counter, ui
 
 // counters[0] += failed, counters[1] += assigned (NULL counters = async form).
 template <class S, int B, bool ASSIGN>
-__global__ void __launch_bounds__(256) k_insert(OaArgs a, void const* pairs, uint8_t const* stencil, uint32_t n,
+__global__ void __launch_bounds__(256) k_insert(__grid_constant__ const OaArgs a, void const* pairs, uint8_t const* stencil, uint32_t n,
                                                 unsigned long long* counters)
 {
     uint32_t failed = 0, assigned = 0;
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) k_insert(OaArgs a, void const* pairs, uin
 // AssignIf (Assign, open_addressing_ref_impl.h:384-410): payload overwrite of
 // existing keys only; an empty slot ends the search.
 template <class S, int B>
-__global__ void __launch_bounds__(256) k_assign_if(OaArgs a, void const* pairs, uint8_t const* stencil, uint32_t n)
+__global__ void __launch_bounds__(256) k_assign_if(__grid_constant__ const OaArgs a, void const* pairs, uint8_t const* stencil, uint32_t n)
 {
     using Raw = typename S::Raw;
     Raw* slots = reinterpret_cast<Raw*>(a.slots);
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) k_assign_if(OaArgs a, void const* pairs, 
 // ----------------------------------------------------------------------------
 
 template <class S, int B>
-__global__ void __launch_bounds__(256) k_iaf_race(OaArgs a, void const* pairs, void* out_found,
+__global__ void __launch_bounds__(256) k_iaf_race(__grid_constant__ const OaArgs a, void const* pairs, void* out_found,
                                                   uint8_t* out_inserted, uint32_t n)
 {
     using Raw = typename S::Raw;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(256) k_iaf_race(OaArgs a, void const* pairs, v
 // ----------------------------------------------------------------------------
 
 template <class S, int B>
-__global__ void __launch_bounds__(256) k_iaf_place(OaArgs a, void const* pairs, uint32_t n, uint32_t* pos,
+__global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArgs a, void const* pairs, uint32_t n, uint32_t* pos,
                                                    uint32_t* newbits, uint32_t* owner)
 {
     using Raw = typename S::Raw;
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t c
 }
 
 template <class S>
-__global__ void __launch_bounds__(256) k_iaf_final(OaArgs a, void const* pairs, uint32_t const* pos,
+__global__ void __launch_bounds__(256) k_iaf_final(__grid_constant__ const OaArgs a, void const* pairs, uint32_t const* pos,
                                                    uint32_t const* newbits, uint32_t const* owner, void* out_found,
                                                    uint8_t* out_inserted, uint32_t n)
 {
@@ -386,17 +386,24 @@ __global__ void __launch_bounds__(256) k_iaf_final(OaArgs a, void const* pairs, 
 // Find / Contains (FindAndContains, open_addressing_ref_impl.h:567-605)
 // ----------------------------------------------------------------------------
 
-// First slot of a loaded window that ends the scan (empty or equal), -1 if none.
+// Whether a loaded window holds a slot that ends the scan (empty or equal); the
+// first such slot is copied into `stop`.  The copy is an unrolled select, so the
+// window stays in registers (indexing it with a computed slot number would move
+// it to local memory).
 template <class S, int B>
-__device__ __forceinline__ int scan_window(typename S::Raw const (&w)[B], uint64_t key, uint64_t empty_key)
+__device__ __forceinline__ bool scan_window(typename S::Raw const (&w)[B], uint64_t key, uint64_t empty_key,
+                                            typename S::Raw& stop)
 {
-    int stop = -1;
+    bool found = false;
 #pragma unroll
     for (int j = B - 1; j >= 0; --j) {
         uint64_t k = S::key(w[j]);
-        if (k == empty_key || k == key) stop = j;
+        if (k == empty_key || k == key) {
+            stop = w[j];
+            found = true;
+        }
     }
-    return stop;
+    return found;
 }
 
 template <class S, int B>
@@ -417,10 +424,10 @@ __device__ __noinline__ bool find_rest(OaArgs const& a, uint64_t key, uint32_t i
     while (idx != init) {
         Raw w[B];
         load_window<S, B>(slots, idx, w);
-        int j = scan_window<S, B>(w, key, a.empty_key);
-        if (j >= 0) {
-            bool hit = S::key(w[j]) != a.empty_key;  // an empty slot ends the scan first
-            payload = hit ? S::value(w[j]) : empty_payload<S>(a);
+        Raw stop;
+        if (scan_window<S, B>(w, key, a.empty_key, stop)) {
+            bool hit = S::key(stop) != a.empty_key;  // an empty slot ends the scan first
+            payload = hit ? S::value(stop) : empty_payload<S>(a);
             return hit;
         }
         idx = probe_next(idx, step, a.probe.capacity);
@@ -432,7 +439,7 @@ __device__ __noinline__ bool find_rest(OaArgs const& a, uint64_t key, uint32_t i
 // One lane per key, ITEMS keys per lane in flight: all windows are loaded
 // before any is resolved, so a lane keeps ITEMS * B independent loads open.
 template <class S, int B, int ITEMS, bool CONTAINS>
-__global__ void __launch_bounds__(256) k_find_lane(OaArgs a, void const* keys, uint8_t const* stencil, void* out,
+__global__ void __launch_bounds__(256) k_find_lane(__grid_constant__ const OaArgs a, void const* keys, uint8_t const* stencil, void* out,
                                                    uint32_t n)
 {
     using Raw = typename S::Raw;
@@ -460,10 +467,10 @@ __global__ void __launch_bounds__(256) k_find_lane(OaArgs a, void const* keys, u
             uint64_t payload = empty_payload<S>(a);
             bool hit = false;
             if (live[t]) {
-                int j = scan_window<S, B>(w[t], key[t], a.empty_key);
-                if (j >= 0) {
-                    hit = S::key(w[t][j]) != a.empty_key;
-                    if (hit) payload = S::value(w[t][j]);
+                Raw stop;
+                if (scan_window<S, B>(w[t], key[t], a.empty_key, stop)) {
+                    hit = S::key(stop) != a.empty_key;
+                    if (hit) payload = S::value(stop);
                 } else {
                     hit = find_rest<S, B>(a, key[t], init[t], payload);
                 }
@@ -478,7 +485,7 @@ __global__ void __launch_bounds__(256) k_find_lane(OaArgs a, void const* keys, u
 // tile resolves the window with one ballot pair per round and the lane holding
 // the hit slot hands its payload to the tile's first lane, which writes it.
 template <class S, int B, int G, bool CONTAINS>
-__global__ void __launch_bounds__(256) k_find_tile(OaArgs a, void const* keys, uint8_t const* stencil, void* out,
+__global__ void __launch_bounds__(256) k_find_tile(__grid_constant__ const OaArgs a, void const* keys, uint8_t const* stencil, void* out,
                                                    uint32_t n)
 {
     using Raw = typename S::Raw;
@@ -519,10 +526,10 @@ __global__ void __launch_bounds__(256) k_find_tile(OaArgs a, void const* keys, u
                     stop_j = __ffs(stop_bits) - 1;
                     hit = (hit_bits >> stop_j) & 1u;
                     done = true;
-                    if (hit && int(r) == stop_j % G) {
+                    if (hit) {
 #pragma unroll
                         for (int t = 0; t < ROUNDS; ++t)
-                            if (t == stop_j / G) payload = S::value(w[t]);
+                            if (int(r) + t * G == stop_j) payload = S::value(w[t]);
                     }
                 } else {
                     if (step == 0) step = probe_step<S::key_bytes, B>(a.probe, key);
@@ -578,12 +585,12 @@ __device__ __forceinline__ void tile_resolve(OaArgs const& a, typename S::Raw co
         hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> lane0) & MASK) << (t * G);
     }
     int const stop_j = stop_bits ? __ffs(stop_bits) - 1 : -1;
+    // the lane holding slot stop_j picks it by a compare per round: a select
+    // keyed on stop_j / G becomes a dynamically indexed copy of w in local memory
     uint64_t mine = 0;
-    if (stop_j >= 0 && int(r) == stop_j % G) {
 #pragma unroll
-        for (int t = 0; t < ROUNDS; ++t)
-            if (t == stop_j / G) mine = S::value(w[t]);
-    }
+    for (int t = 0; t < ROUNDS; ++t)
+        if (int(r) + t * G == stop_j) mine = S::value(w[t]);
     uint64_t const got = __shfl_sync(0xffffffffu, (unsigned long long)mine, lane0 + (stop_j >= 0 ? stop_j % G : 0));
     if (!skip && stop_j >= 0) {
         res.done = true;
@@ -592,10 +599,10 @@ __device__ __forceinline__ void tile_resolve(OaArgs const& a, typename S::Raw co
     }
 }
 
-// Line-split scan of a first window (the SEG variant).  DRAM reads for random
-// lookups arrive as whole 128-byte L2 lines, and an 80-byte bucket straddles two
-// lines half of the time; the split variant reads the part in the first line,
-// and the part in the second line only for windows the first part did not
+// Split scan of a first window (the SEG variant).  DRAM reads for random
+// lookups arrive as whole fill units (64 bytes under ld_ro's hint), and an
+// 80-byte bucket spans two or three of them; the split variant reads the part
+// in the first unit, and the rest only for windows the first part did not
 // settle.
 //
 // Slots [lo, hi) of a window, lane r holding slots lo + r + t*G (t < ROUNDS):
@@ -627,11 +634,9 @@ __device__ __forceinline__ void resolve_range(OaArgs const& a, typename S::Raw c
     }
     int const s = stop_bits ? __ffs(stop_bits) - 1 : -1;
     uint64_t mine = 0;
-    if (s >= 0 && int(r) == s % G) {
 #pragma unroll
-        for (int t = 0; t < ROUNDS; ++t)
-            if (t == s / G) mine = S::value(w[t]);
-    }
+    for (int t = 0; t < ROUNDS; ++t)
+        if (int(r) + t * G == s) mine = S::value(w[t]);
     uint64_t const got = __shfl_sync(0xffffffffu, (unsigned long long)mine, lane0 + (s >= 0 ? s % G : 0));
     if (!skip && s >= 0) {
         res.done = true;
@@ -640,11 +645,14 @@ __device__ __forceinline__ void resolve_range(OaArgs const& a, typename S::Raw c
     }
 }
 
-// Slots of the window starting at `idx` before the next 128-byte L2 line boundary.
+// DRAM fill unit of the read-only loads: ld_ro asks for 64-byte L2 fills.
+constexpr int kFillBytes = 64;
+
+// Slots of the window starting at `idx` before the next fill-unit boundary.
 template <class S, int B>
 __device__ __forceinline__ int slots_to_line_end(uint32_t idx)
 {
-    constexpr int per = 128 / S::bytes;
+    constexpr int per = kFillBytes / S::bytes;
     int const n1 = per - int(idx % per);
     return n1 < B ? n1 : B;
 }
@@ -653,7 +661,7 @@ __device__ __forceinline__ int slots_to_line_end(uint32_t idx)
 // empty slot (rare at load factor 0.5); the whole warp iterates until every
 // tile is done.
 template <class S, int B, int G, int ROUNDS>
-__device__ __noinline__ TileResult tile_continue(OaArgs a, typename S::Raw const* slots, uint64_t key, uint32_t init,
+__device__ __forceinline__ TileResult tile_continue(OaArgs a, typename S::Raw const* slots, uint64_t key, uint32_t init,
                                                  uint32_t r, uint32_t lane0, TileResult res)
 {
     uint32_t idx = init, step = 0;
@@ -677,7 +685,7 @@ __device__ __noinline__ TileResult tile_continue(OaArgs a, typename S::Raw const
 }
 
 template <class S, int B, int G, int Q, bool CONTAINS, bool SEG>
-__global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
+__global__ void __launch_bounds__(256) k_find_staged(__grid_constant__ const OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
 {
     static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");
     using Raw = typename S::Raw;
@@ -839,7 +847,7 @@ __global__ void __launch_bounds__(256) k_find_staged(OaArgs a, void const* keys,
 constexpr uint32_t kWarpStageKeys = 256;
 
 template <class S, int B, int G, int Q, bool CONTAINS>
-__global__ void __launch_bounds__(256) k_find_wstaged(OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
+__global__ void __launch_bounds__(256, 4) k_find_wstaged(__grid_constant__ const OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
 {
     static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");
     using Raw = typename S::Raw;
@@ -970,7 +978,7 @@ __host__ __device__ constexpr uint32_t bulk_window_smem()
 }
 
 template <class S, int B, bool CONTAINS>
-__global__ void __launch_bounds__(256) k_find_bulk(OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
+__global__ void __launch_bounds__(256) k_find_bulk(__grid_constant__ const OaArgs a, void const* keys, void* out, uint32_t n, WaitCtl wc)
 {
     static_assert(S::bytes == 16, "bulk windows need 16-byte slots (16-byte aligned windows)");
     using Raw = typename S::Raw;
@@ -1086,12 +1094,12 @@ __global__ void __launch_bounds__(256) k_find_bulk(OaArgs a, void const* keys, v
             uint32_t const init0 = probe_init<S::key_bytes, B>(a.probe, key);
             Raw w[B];
             load_window<S, B>(slots, init0, w);
-            int j = scan_window<S, B>(w, key, a.empty_key);
+            Raw stop;
             uint64_t payload = empty_payload<S>(a);
             bool hit;
-            if (j >= 0) {
-                hit = S::key(w[j]) != a.empty_key;
-                if (hit) payload = S::value(w[j]);
+            if (scan_window<S, B>(w, key, a.empty_key, stop)) {
+                hit = S::key(stop) != a.empty_key;
+                if (hit) payload = S::value(stop);
             } else {
                 hit = find_rest<S, B>(a, key, init0, payload);
             }
@@ -1106,7 +1114,7 @@ __global__ void __launch_bounds__(256) k_find_bulk(OaArgs a, void const* keys, v
 // ----------------------------------------------------------------------------
 
 template <class S, int B>
-__global__ void __launch_bounds__(256) k_erase(OaArgs a, void const* keys, uint32_t n, unsigned long long* counters)
+__global__ void __launch_bounds__(256) k_erase(__grid_constant__ const OaArgs a, void const* keys, uint32_t n, unsigned long long* counters)
 {
     using Raw = typename S::Raw;
     Raw* slots = reinterpret_cast<Raw*>(a.slots);
@@ -1157,7 +1165,7 @@ __global__ void __launch_bounds__(256) k_erase(OaArgs a, void const* keys, uint3
 }
 
 template <class S, int B>
-__global__ void __launch_bounds__(256) k_count(OaArgs a, void const* keys, uint32_t n, unsigned long long* counter)
+__global__ void __launch_bounds__(256) k_count(__grid_constant__ const OaArgs a, void const* keys, uint32_t n, unsigned long long* counter)
 {
     using Raw = typename S::Raw;
     Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
@@ -1170,9 +1178,9 @@ __global__ void __launch_bounds__(256) k_count(OaArgs a, void const* keys, uint3
         uint32_t init = probe_init<S::key_bytes, B>(a.probe, key);
         Raw w[B];
         load_window<S, B>(slots, init, w);
-        int j = scan_window<S, B>(w, key, a.empty_key);
+        Raw stop;
         uint64_t payload;
-        if (j >= 0) c += S::key(w[j]) != a.empty_key;
+        if (scan_window<S, B>(w, key, a.empty_key, stop)) c += S::key(stop) != a.empty_key;
         else c += find_rest<S, B>(a, key, init, payload);
     }
     warp_add_counter(counter, c);
