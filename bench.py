@@ -212,14 +212,16 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 
 def parse_shape(s: str):
-    """'LxK', 'LxKs' or 'bulk': L lanes per key, K keys in flight per lane group,
-    s = segmented windows, bulk = one bulk copy per bucket window."""
+    """'LxK', 'LxKs', 'LxKw', 'LxKd' or 'bulk': L lanes per key, K keys in flight
+    per lane group; s = segmented windows, w = keys staged per warp, d = per-warp
+    staging with deferred continuations, bulk = one bulk copy per bucket window."""
     if s == "bulk":
-        return 1, 1, False, True, False
+        return 1, 1, False, True, False, False
     warp = s.endswith("w")
     seg = s.endswith("s")
-    lanes, items = (int(x) for x in s.rstrip("sw").split("x"))
-    return lanes, items, seg, False, warp
+    defer = s.endswith("d")
+    lanes, items = (int(x) for x in s.rstrip("swd").split("x"))
+    return lanes, items, seg, False, warp, defer
 
 
 def peaks():
@@ -312,7 +314,7 @@ def run_gpu(args):
     if args.sweep:
         sweep = {}
         shapes = args.sweep_shapes.split(",") if args.sweep_shapes else [
-            "2x2", "2x2w", "2x1w", "4x1w", "4x2w", "4x4w", "8x4w", "4x2", "2x2s"]
+            "4x2d", "2x2d", "4x1d", "8x2d", "2x2w", "4x2w", "2x2", "4x2", "2x2s"]
         for shape in shapes:
             t.set_find_shape(*parse_shape(shape))
             for _ in range(3):
@@ -377,7 +379,8 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD, "capacity": cap, "unique_keys": unique, "insert_stream": unique + dups,
                        "queries": N_QUERIES, "hit_rate": 0.5, "bucket_size": 5, "probing": "DoubleHashing<xxhash_32>",
                        "l2": "inputs larger than L2 (4.3 GB table + 1 GB keys)", "parallelism": f"replicas x{world}",
-                       "find_shape": args.shape or "default"},
+                       "find_shape": args.shape or "default (4x2d: 4 lanes per window, 2 windows in flight, "
+                                     "per-warp key staging, deferred continuations)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
             "clocks": clk.summary(), "fill_ms": round(fill_ms, 2), "extra": extra,
         }

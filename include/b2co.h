@@ -203,6 +203,9 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
 #define B2CO_FIND_BULK 0x200u
 /* OR-ed into keys_per_lane: every warp stages its own key chunks (no block barrier). */
 #define B2CO_FIND_WARP_STAGED 0x400u
+/* OR-ed into keys_per_lane: warp-staged keys, and keys whose first bucket window
+ * does not settle them are queued and followed a whole pass at a time. */
+#define B2CO_FIND_DEFERRED 0x800u
 int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_lane);
 
 /* ===================================================================== */

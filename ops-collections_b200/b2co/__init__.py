@@ -33,6 +33,7 @@ INSERT_EXACT_DEDUP, INSERT_APPEND_UNIQUE = 0, 1
 FIND_SEGMENTED = 0x100
 FIND_BULK = 0x200
 FIND_WARP_STAGED = 0x400
+FIND_DEFERRED = 0x800
 
 
 class B2coError(Exception):
@@ -312,9 +313,9 @@ class _OaBase:
               C.c_uint64(n), _stream(stream))
 
     def set_find_shape(self, lanes_per_key: int, keys_per_lane: int, segmented: bool = False, bulk: bool = False,
-                       warp_staged: bool = False):
+                       warp_staged: bool = False, deferred: bool = False):
         flags = (FIND_SEGMENTED if segmented else 0) | (FIND_BULK if bulk else 0) | \
-            (FIND_WARP_STAGED if warp_staged else 0)
+            (FIND_WARP_STAGED if warp_staged else 0) | (FIND_DEFERRED if deferred else 0)
         _call("b2co_oa_set_find_shape", self._h, C.c_uint32(lanes_per_key), C.c_uint32(keys_per_lane | flags))
 
     @staticmethod

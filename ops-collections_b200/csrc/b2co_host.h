@@ -53,6 +53,9 @@ constexpr uint32_t kShapeSegmented = 0x100;
 constexpr uint32_t kShapeBulk = 0x200;
 // Lookup shape flag: every warp stages its own keys (B2CO_FIND_WARP_STAGED).
 constexpr uint32_t kShapeWarpStaged = 0x400;
+// Lookup shape flag: warp-staged keys whose first window does not settle them
+// are queued and followed a pass at a time (B2CO_FIND_DEFERRED).
+constexpr uint32_t kShapeDeferred = 0x800;
 
 // Launchers for one slot layout; B (bucket size) is dispatched at run time.
 struct OaOps {

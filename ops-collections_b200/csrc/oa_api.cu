@@ -75,11 +75,13 @@ void default_shape(b2co_oa_table* t)
         t->find_lanes = 1;  // a one-slot window needs no cooperation
         t->find_items = 4;
     } else {
-        // keys staged per warp (no block barrier: a warp whose keys need further
-        // windows holds up no other warp), two lanes per bucket window, two
-        // windows in flight per pair
-        t->find_lanes = 2;
-        t->find_items = 2 | kShapeWarpStaged;
+        // keys staged per warp, keys that probe on past their first window
+        // queued and followed a pass at a time; four lanes per window (a 64-byte
+        // row of 16-byte slots per load) with two windows in flight, or two
+        // lanes and one window for 4-byte slots (measured best per layout)
+        bool const narrow = slot_bytes(t->desc.key_bytes, t->desc.value_bytes) == 4;
+        t->find_lanes = narrow ? 2 : 4;
+        t->find_items = (narrow ? 1 : 2) | kShapeDeferred;
     }
 }
 
@@ -506,7 +508,7 @@ int b2co_oa_set_find_shape(b2co_oa_table* t, uint32_t lanes, uint32_t items)
         return B2CO_OK;
     }
     if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) return fail(B2CO_EINVAL, "lanes must be 1, 2, 4 or 8");
-    uint32_t const k = items & ~(kShapeSegmented | kShapeBulk | kShapeWarpStaged);
+    uint32_t const k = items & ~(kShapeSegmented | kShapeBulk | kShapeWarpStaged | kShapeDeferred);
     if (k != 1 && k != 2 && k != 4) return fail(B2CO_EINVAL, "keys per lane must be 1, 2 or 4");
     t->find_lanes = lanes;
     t->find_items = items;

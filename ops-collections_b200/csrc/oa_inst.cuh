@@ -117,6 +117,20 @@ struct OaImpl {
         return check_launch(C ? "contains kernel" : "find kernel");
     }
 
+    template <int B, int G, bool C>
+    static int find_wdefer(OaArgs const& a, uint32_t items, void const* keys, void* out, uint32_t n, WaitCtl wc,
+                           cudaStream_t s)
+    {
+        void (*k)(OaArgs, void const*, void*, uint32_t, WaitCtl) = nullptr;
+        if (items >= 4 && G >= 4) k = k_find_wdefer<S, B, G, (G >= 4 ? 4 : 1), C>;
+        else if (items >= 2) k = k_find_wdefer<S, B, G, 2, C>;
+        else k = k_find_wdefer<S, B, G, 1, C>;
+        uint64_t warps = (n + kWarpStageKeys - 1) / kWarpStageKeys;
+        uint32_t grid = grid_for((void const*)k, kBlock, warps ? warps : 1, kBlock / 32);
+        k<<<grid, kBlock, 0, s>>>(a, keys, out, n, wc);
+        return check_launch(C ? "contains kernel" : "find kernel");
+    }
+
     template <int B, bool C>
     static int find_bulk(OaArgs const& a, void const* keys, void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
     {
@@ -152,6 +166,13 @@ struct OaImpl {
         items &= ~kShapeBulk;
         // staged path: no stencil, 16-byte aligned key stream, at least one stage of keys
         bool const staged = stageable && lanes >= 2;
+        if (staged && (items & kShapeDeferred)) {
+            items &= ~(kShapeDeferred | kShapeWarpStaged | kShapeSegmented);
+            if (lanes == 2) return find_wdefer<B, 2, C>(a, items, keys, out, n, wc, s);
+            if (lanes == 4) return find_wdefer<B, 4, C>(a, items, keys, out, n, wc, s);
+            return find_wdefer<B, 8, C>(a, items, keys, out, n, wc, s);
+        }
+        items &= ~kShapeDeferred;
         if (staged && (items & kShapeWarpStaged)) {
             items &= ~(kShapeWarpStaged | kShapeSegmented);
             if (lanes == 2) return find_wstaged<B, 2, C>(a, items, keys, out, n, wc, s);

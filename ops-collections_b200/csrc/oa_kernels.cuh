@@ -959,6 +959,232 @@ __global__ void __launch_bounds__(256, 4) k_find_wstaged(__grid_constant__ const
 }
 
 // ----------------------------------------------------------------------------
+// Deferred-continuation lookups: keys staged per warp as in k_find_wstaged, but
+// a key whose first window holds neither the key nor an empty slot is queued in
+// the warp's shared-memory ring instead of being followed at once, so a pass
+// costs one dependent window load however many of its keys probe on.  Once a
+// whole pass of keys is queued the warp follows them together, one window each,
+// and queues again the few that need yet another.  A tile resolves a window
+// without ballots: each lane finds the first slot among its own that ends the
+// scan, a min over the tile's lanes gives the window's first, and the lane
+// holding that slot writes the result.
+// ----------------------------------------------------------------------------
+
+constexpr uint32_t kDeferRing = 64;  // queued keys per warp (a power of two)
+constexpr int kNoStop = 255;
+
+// First slot of a window (lane r holds slots r + t*G) that ends the scan of
+// `key`, agreed by the tile's G lanes, or kNoStop.  `own` is the lane's own
+// first such slot (kNoStop if none) and `mine` that slot's contents.  Lanes of
+// tiles with `skip` set only take part in the shuffles.
+template <class S, int B, int G, int ROUNDS>
+__device__ __forceinline__ int tile_first_stop(typename S::Raw const (&w)[ROUNDS], bool skip, uint64_t key,
+                                               uint64_t empty_key, uint32_t r, int& own, typename S::Raw& mine)
+{
+    own = kNoStop;
+#pragma unroll
+    for (int t = ROUNDS - 1; t >= 0; --t) {
+        if (!skip && int(r) + t * G < B) {
+            uint64_t const k = S::key(w[t]);
+            if (k == empty_key || k == key) {
+                own = int(r) + t * G;
+                mine = w[t];
+            }
+        }
+    }
+    int s = own;
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) s = min(s, __shfl_xor_sync(0xffffffffu, s, o));
+    return s;
+}
+
+template <class S, int B, int G, int Q, bool CONTAINS>
+__global__ void __launch_bounds__(256, Q == 1 ? 4 : 3) k_find_wdefer(__grid_constant__ const OaArgs a, void const* keys, void* out,
+                                                        uint32_t n, WaitCtl wc)
+{
+    static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");
+    using Raw = typename S::Raw;
+    using Key = typename Io<S>::Key;
+    constexpr int ROUNDS = (B + G - 1) / G;
+    constexpr uint32_t TILES = 32 / G;   // tiles per warp
+    constexpr uint32_t PASS = TILES * Q;  // keys per warp pass
+    static_assert(kWarpStageKeys % PASS == 0, "stage must hold whole passes");
+    static_assert(2 * PASS <= kDeferRing, "the ring must hold a pass on top of a partial one");
+    constexpr uint32_t RING = kDeferRing - 1;
+    constexpr uint32_t kChunkBytes = kWarpStageKeys * sizeof(Key);
+    __shared__ alignas(128) Key sk[8][2][kWarpStageKeys];
+    __shared__ alignas(8) uint64_t bar[8][2];
+    __shared__ alignas(8) uint64_t never[8];
+    // the warp's queue of keys still probing: key, first window, last window read, output index
+    __shared__ uint64_t qkey[8][kDeferRing];
+    __shared__ uint32_t qinit[8][kDeferRing], qidx[8][kDeferRing], qpos[8][kDeferRing];
+
+    Raw const* slots = reinterpret_cast<Raw const*>(a.slots);
+    uint32_t const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t const r = lane % G, tile_lane0 = lane & ~uint32_t(G - 1), tile = lane / G;
+    uint32_t const gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    uint32_t const nwarps = (gridDim.x * blockDim.x) >> 5;
+    uint32_t const chunks = n / kWarpStageKeys;
+    Key const* kin = static_cast<Key const*>(keys);
+    uint32_t head = 0, count = 0;  // queue state, the same on every lane
+
+    auto settle = [&](uint32_t pos, Raw const& slot) {  // result from the slot that ended the scan
+        bool const hit = S::key(slot) != a.empty_key;
+        if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[pos] = hit;
+        else Io<S>::store_payload(out, pos, hit ? S::value(slot) : empty_payload<S>(a));
+    };
+    auto settle_miss = [&](uint32_t pos) {
+        if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[pos] = 0;
+        else Io<S>::store_payload(out, pos, empty_payload<S>(a));
+    };
+    // Lane 0 of each tile whose window ended no scan queues its key.
+    auto enqueue = [&](bool unsettled, uint64_t key, uint32_t init, uint32_t idx, uint32_t pos) {
+        uint32_t const m = __ballot_sync(0xffffffffu, unsettled);
+        if (unsettled) {
+            uint32_t const e = (head + count + __popc(m & ((1u << lane) - 1u))) & RING;
+            qkey[warp][e] = key;
+            qinit[warp][e] = init;
+            qidx[warp][e] = idx;
+            qpos[warp][e] = pos;
+        }
+        count += __popc(m);
+    };
+    // Takes up to one pass of queued keys and reads the next window of each.
+    auto follow = [&]() {
+        __syncwarp();  // the queue writes precede these reads
+        uint32_t const take = count < PASS ? count : PASS;
+        uint64_t key[Q];
+        uint32_t init[Q], idx[Q], pos[Q];
+        bool live[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t const j = q * TILES + tile;
+            live[q] = j < take;
+            uint32_t const e = (head + (live[q] ? j : 0u)) & RING;
+            key[q] = qkey[warp][e];
+            init[q] = qinit[warp][e];
+            idx[q] = qidx[warp][e];
+            pos[q] = qpos[warp][e];
+        }
+        __syncwarp();  // every read of the taken entries precedes their reuse
+        head = (head + take) & RING;
+        count -= take;
+        uint32_t my_step = 0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (int(r) == q && live[q]) my_step = probe_step<S::key_bytes, B>(a.probe, key[q]);
+        Raw w[Q][ROUNDS];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t const step = __shfl_sync(0xffffffffu, my_step, tile_lane0 + q);
+            if (live[q]) {
+                idx[q] = probe_next(idx[q], step, a.probe.capacity);
+                if (idx[q] == init[q]) {  // full cycle: not present
+                    if (r == 0) settle_miss(pos[q]);
+                    live[q] = false;
+                }
+            }
+            load_range<S, B, G, ROUNDS>(slots, idx[q], 0, B, r, !live[q], w[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            int own;
+            Raw mine{};
+            int const s = tile_first_stop<S, B, G, ROUNDS>(w[q], !live[q], key[q], a.empty_key, r, own, mine);
+            if (live[q] && s != kNoStop && own == s) settle(pos[q], mine);
+            enqueue(live[q] && s == kNoStop && r == 0, key[q], init[q], idx[q], pos[q]);
+        }
+    };
+
+    if (lane == 0) {
+        mbar_init(&bar[warp][0], 1);
+        mbar_init(&bar[warp][1], 1);
+        mbar_init(&never[warp], 1);
+        fence_mbar_init();
+        if (gwarp < chunks) {
+            mbar_arrive_expect_tx(&bar[warp][0], kChunkBytes);
+            bulk_g2s(sk[warp][0], kin + uint64_t(gwarp) * kWarpStageKeys, kChunkBytes, &bar[warp][0]);
+        }
+    }
+    __syncwarp();
+    uint32_t it = 0;
+    bool failed = false;
+    for (uint32_t c = gwarp; c < chunks; c += nwarps, ++it) {
+        uint32_t const b = it & 1;
+        uint32_t const cn = c + nwarps;
+        if (lane == 0 && cn < chunks) {
+            fence_proxy_async();  // the warp's reads of this buffer (previous chunk) precede the copy
+            mbar_arrive_expect_tx(&bar[warp][b ^ 1], kChunkBytes);
+            bulk_g2s(sk[warp][b ^ 1], kin + uint64_t(cn) * kWarpStageKeys, kChunkBytes, &bar[warp][b ^ 1]);
+        }
+        bool const ok = wc.probe_timeout ? mbar_wait_bounded(&never[warp], 0, wc.ns)
+                                         : mbar_wait_bounded(&bar[warp][b], (it >> 1) & 1, wc.ns);
+        if (__any_sync(0xffffffffu, !ok)) {
+            failed = true;
+            break;
+        }
+        Key const* ks = sk[warp][b];
+        uint32_t const base = c * kWarpStageKeys;
+        for (uint32_t p = 0; p < kWarpStageKeys; p += PASS) {
+            uint64_t key[Q];
+            uint32_t idx[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) key[q] = ks[p + q * TILES + tile];
+            uint32_t my_init = 0;
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                if (int(r) == q) my_init = probe_init<S::key_bytes, B>(a.probe, key[q]);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) idx[q] = __shfl_sync(0xffffffffu, my_init, tile_lane0 + q);
+            Raw w[Q][ROUNDS];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) load_range<S, B, G, ROUNDS>(slots, idx[q], 0, B, r, false, w[q]);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                int own;
+                Raw mine{};
+                int const s = tile_first_stop<S, B, G, ROUNDS>(w[q], false, key[q], a.empty_key, r, own, mine);
+                uint32_t const i = base + p + q * TILES + tile;
+                if (s != kNoStop && own == s) settle(i, mine);
+                enqueue(s == kNoStop && r == 0, key[q], idx[q], idx[q], i);
+            }
+            while (count >= PASS) follow();
+        }
+        __syncwarp();  // every lane is done with this buffer before it is refilled
+    }
+    if (failed) {
+        if (lane == 0) {
+            atomicExch(wc.status, kStatusTimeout);
+            // let this warp's copies still in flight land before the block can exit (bounded again)
+            uint32_t const c = gwarp + it * nwarps;
+            mbar_wait_bounded(&bar[warp][it & 1], (it >> 1) & 1, 1000000000ull);
+            if (c + nwarps < chunks) mbar_wait_bounded(&bar[warp][(it + 1) & 1], ((it + 1) >> 1) & 1, 1000000000ull);
+        }
+        return;
+    }
+    while (count > 0) follow();  // each round moves every queued key on by a window or settles it
+    // the ragged tail (< one warp stage) goes to one warp, keys read directly
+    if (chunks * kWarpStageKeys < n && gwarp == chunks % nwarps) {
+        for (uint32_t i0 = chunks * kWarpStageKeys; i0 < n; i0 += TILES) {
+            uint32_t const i = i0 + tile;
+            bool const live = i < n;
+            uint64_t const key = live ? Io<S>::load_key(keys, i) : 0;
+            uint32_t const init0 = live ? probe_init<S::key_bytes, B>(a.probe, key) : 0;
+            Raw w[ROUNDS];
+            load_range<S, B, G, ROUNDS>(slots, init0, 0, B, r, !live, w);
+            TileResult res{0, false, !live};
+            resolve_range<S, B, G, ROUNDS>(a, w, 0, B, key, r, tile_lane0, !live, res);
+            if (__any_sync(0xffffffffu, !res.done))
+                res = tile_continue<S, B, G, ROUNDS>(a, slots, key, init0, r, tile_lane0, res);
+            if (r == 0 && live) {
+                if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = res.hit;
+                else Io<S>::store_payload(out, i, res.hit ? res.payload : empty_payload<S>(a));
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
 // Bulk-window lookups (16-byte slots): every lane fetches its key's whole first
 // bucket window (B x 16 bytes, 16-byte aligned) with ONE bulk copy (TMA,
 // untiled) into shared memory.  Copies are tracked by the SM's bulk-copy

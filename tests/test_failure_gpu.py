@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("shape", [(8, 4, False, False, False), (1, 1, False, True, False),
-                                   (2, 2, False, False, True)], ids=["staged", "bulk", "warp_staged"])
+                                   (2, 2, False, False, True), (2, 2, False, False, False, True)],
+                         ids=["staged", "bulk", "warp_staged", "deferred"])
 def test_bounded_wait_reports_timeout_and_context_survives(shape):
     import b2co
     import torch

@@ -234,6 +234,35 @@ def test_full_table(layout):
     assert t.Count(dev(miss_keys(rng, 50, kb))) == 0
 
 
+@pytest.mark.parametrize("layout", [(4, 4), (8, 8), (8, 0)], ids=lambda l: f"k{l[0]}v{l[1]}")
+def test_staged_shapes_on_full_table(layout):
+    """Staged lookups of a full table: a miss follows every window of its probe
+    cycle (the deferred shape queues it again window after window until the
+    cycle closes), hits settle anywhere along the way.  Checked against the
+    oracle reading the device table's own slots."""
+    import torch
+    kb, vb = layout
+    b, probing, hk = SCHEMES[0]
+    rng = np.random.default_rng(21)
+    t = make_table(kb, vb, b, probing, hk, 300)
+    keys = unique_keys(rng, t.Capacity() + 40, kb)
+    t.Insert(make_pairs(keys, values_for(rng, keys, vb)))
+    _, o = stored_pairs(t, kb, vb, b, probing, hk)
+    q = np.concatenate([keys, miss_keys(rng, 3000, kb)])
+    rng.shuffle(q)
+    qd = dev(q)
+    ref = (o.find(q)[0], o.contains(q)[0])
+    for shape in [(2, 2, False, False, False, True), (4, 4, False, False, False, True),
+                  (8, 1, False, False, False, True), (2, 2, False, False, True, False), (2, 2, False, False, False, False)]:
+        t.set_find_shape(*shape)
+        out = out_buf(len(q), kb, vb)
+        t.Find(qd, out)
+        c = torch.empty(len(q), dtype=torch.uint8, device="cuda")
+        t.Contains(qd, c)
+        assert np.array_equal(out.cpu().numpy(), ref[0]), shape
+        assert np.array_equal(c.cpu().numpy(), ref[1]), shape
+
+
 def test_edge_cases_and_errors():
     import b2co
     import torch
@@ -269,11 +298,13 @@ def test_find_shapes_agree():
         o = oracle_table(t, kb, vb, b, oracle.PROBE_DOUBLE, oracle.HASH_XXH32)
         o.insert(keys, vals)
         ref = (o.find(q)[0], o.contains(q)[0])
-        shapes = [(l, i, False, False, False) for l in (1, 2, 4, 8) for i in (1, 2, 4)] + \
-                 [(l, i, True, False, False) for l in (2, 4, 8) for i in (1, 2, 4)] + \
-                 [(l, i, False, False, True) for l in (2, 4, 8) for i in (1, 2, 4)] + [(1, 1, False, True, False)]
-        for lanes, items, seg, bulk, warp in shapes:
-            t.set_find_shape(lanes, items, seg, bulk, warp)
+        shapes = [(l, i, False, False, False, False) for l in (1, 2, 4, 8) for i in (1, 2, 4)] + \
+                 [(l, i, True, False, False, False) for l in (2, 4, 8) for i in (1, 2, 4)] + \
+                 [(l, i, False, False, True, False) for l in (2, 4, 8) for i in (1, 2, 4)] + \
+                 [(l, i, False, False, False, True) for l in (2, 4, 8) for i in (1, 2, 4)] + \
+                 [(1, 1, False, True, False, False)]
+        for lanes, items, seg, bulk, warp, defer in shapes:
+            t.set_find_shape(lanes, items, seg, bulk, warp, defer)
             out = out_buf(len(q), kb, vb)
             t.Find(qd, out)
             c = torch.empty(len(q), dtype=torch.uint8, device="cuda")
