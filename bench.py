@@ -365,6 +365,7 @@ def run_gpu(args):
                 "peak_source": peak_kind, "bytes_per_query": round(bytes_per_query, 3),
                 "windows_per_query": windows_mean,
                 "one_window_bound_gbs": round(N_QUERIES * 96 / (ms_per_step / 1e3) / 1e9, 1)}
+    roofline.update(window_gather_ceiling(t, stream, value, windows_mean))
 
     e2e = None if args.no_e2e else measure_e2e(t, q, out, stream, world, args)
 
@@ -410,6 +411,30 @@ def measure_e2e(t, q, out, stream, world, args):
     return {"value": round(world * N_QUERIES / (e2e_ms / 1e3) / 1e9, 4), "unit": UNIT,
             "h2d_bytes_per_step": N_QUERIES * 8, "d2h_bytes_per_step": N_QUERIES * 8,
             "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 24) - 1) >> 24}
+
+
+def window_gather_ceiling(t, stream, find_gkeys, windows_mean):
+    """The random bucket-window read rate of this GPU over the very same table:
+    bare reads of whole 80-byte windows at random bucket starts, none of a
+    lookup's other work (key stream, hashing, outputs, second windows).  Random
+    80-byte windows move whole DRAM fill units, so this rate, not the copy peak,
+    is what Find can approach; timed after (never inside) the Find region."""
+    import torch
+    n = 1 << 27
+    for i in range(3):
+        t.window_gather(n, seed=11 + i, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(10):
+        t.window_gather(n, seed=101 + i, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    gwin = n * 10 / (e0.elapsed_time(e1) / 1e3) / 1e9
+    out = {"window_gather_ceiling_gwin": round(gwin, 3)}
+    if windows_mean:
+        out["find_windows_vs_ceiling"] = round(find_gkeys * windows_mean / gwin, 4)
+    return out
 
 
 def host_side_checks(t, q, out, args):

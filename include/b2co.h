@@ -113,6 +113,12 @@ int b2co_oa_data(const b2co_oa_table* table, void** slots);
  * containers expose the same through their template parameters and
  * constructor arguments (static_map.h:78-84). */
 int b2co_oa_describe(const b2co_oa_table* table, b2co_oa_desc* desc);
+/* Measurement aid (no reference counterpart): `n` (<= 2^31) reads of whole
+ * bucket windows at pseudo-random bucket starts (`seed`) of the table's own
+ * slots, four lanes per window, nothing written.  16-byte slots only.  Timing it
+ * gives the random-window read rate a lookup's first windows can reach on this
+ * GPU, the practical ceiling of Find beside the HBM copy peak. */
+int b2co_oa_window_gather(const b2co_oa_table* table, uint64_t n, uint32_t seed, b2co_stream stream);
 /* reference: static_map.h:97 SetErasedKey (static_map.inl:59-66). */
 int b2co_oa_set_erased_key(b2co_oa_table* table, uint64_t erased_key_bits, b2co_stream stream);
 /* reference: static_map.h:318 Clear, :331 ClearAsync. */

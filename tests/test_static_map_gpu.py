@@ -328,3 +328,23 @@ def test_find_host_buffers_match_device_find():
     out = out_buf(len(q), 8, 8)
     t.Find(dev(q), out)
     assert np.array_equal(pinned_o.numpy(), out.cpu().numpy())
+
+
+def test_window_gather_measurement_aid():
+    """The bare window-read measurement runs over 16-byte-slot tables only,
+    leaves the table unchanged and keeps the batch bound."""
+    import b2co
+    import torch
+    rng = np.random.default_rng(4)
+    t = make_table(8, 8, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, 1 << 16)
+    keys = unique_keys(rng, 20000, 8)
+    t.Insert(make_pairs(keys, keys))
+    before = t.dump_slots()
+    t.window_gather(1 << 20, seed=3)
+    torch.cuda.synchronize()
+    assert np.array_equal(t.dump_slots(), before)
+    with pytest.raises(b2co.LengthError):
+        t.window_gather((1 << 31) + 1)
+    s = make_table(8, 0, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, 1 << 12)
+    with pytest.raises(b2co.InvalidArgument):
+        s.window_gather(1024)
