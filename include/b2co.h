@@ -200,9 +200,10 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
 /* Kernel shape used by Find/Contains on this table: lanes per key (1, 2, 4 or
  * 8) and keys in flight per lane group (1, 2 or 4), optionally OR-ed with
  * B2CO_FIND_SEGMENTED (scan each first bucket window by 64-byte segments and
- * read the second segment only when the first does not end the scan); 0, 0 =
- * library default.  The autotuner sets these.  No reference counterpart (the
- * reference launches one thread per key). */
+ * read the second segment only when the first does not end the scan) and the
+ * flags below; 0, 0 = library default (4 lanes, 2 windows, B2CO_FIND_DEFERRED;
+ * 2 lanes, 1 window for 4-byte slots).  No reference counterpart (the reference
+ * launches one thread per key). */
 #define B2CO_FIND_SEGMENTED 0x100u
 /* OR-ed into keys_per_lane: fetch every first bucket window with one bulk (TMA)
  * copy into shared memory; tables with 16-byte slots only (others ignore it). */
