@@ -410,7 +410,7 @@ def measure_e2e(t, q, out, stream, world, args):
     assert torch.equal(ho, out.cpu()), "host-buffer Find differs from device Find"
     return {"value": round(world * N_QUERIES / (e2e_ms / 1e3) / 1e9, 4), "unit": UNIT,
             "h2d_bytes_per_step": N_QUERIES * 8, "d2h_bytes_per_step": N_QUERIES * 8,
-            "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 24) - 1) >> 24}
+            "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 22) - 1) >> 22}
 
 
 def window_gather_ceiling(t, stream, find_gkeys, windows_mean):

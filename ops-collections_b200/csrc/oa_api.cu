@@ -12,6 +12,9 @@
 
 using namespace b2co;
 
+// Staging slots (and pipeline streams) of the host-buffer Find.
+constexpr int kHostSlots = 3;
+
 struct b2co_oa_table {
     b2co_oa_desc desc{};
     OaArgs args{};
@@ -28,8 +31,8 @@ struct b2co_oa_table {
     // host-buffer Find pipeline
     void* stage = nullptr;
     uint64_t stage_keys = 0;
-    cudaStream_t pipe[2] = {nullptr, nullptr};
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t pipe[kHostSlots] = {};
+    cudaEvent_t ev[kHostSlots + 1] = {};  // per-stream completion, then the caller's start
     uint32_t find_lanes = 0, find_items = 0;
 };
 
@@ -588,29 +591,32 @@ int b2co_oa_set_find_shape(b2co_oa_table* t, uint32_t lanes, uint32_t items)
     return B2CO_OK;
 }
 
-// Host-buffer Find: chunks alternate between two pipeline streams, each chunk
-// copy-in -> probe -> copy-out in stream order, so chunk c+1's copy-in overlaps
-// chunk c's probe and copy-out.  Pinned host buffers give full overlap.
+// Host-buffer Find: chunks of 4 Mi keys rotate over kHostSlots staging slots,
+// one pipeline stream per slot, each chunk copy-in -> probe -> copy-out in its
+// stream.  Consecutive chunks sit on different streams, so later chunks copy in
+// while earlier ones probe and copy out and both copy directions stay busy;
+// small chunks keep the unoverlapped first copy-in and last copy-out short.
+// Pinned host buffers give full overlap.
 int b2co_oa_find_host(b2co_oa_table* t, void const* host_keys, void* host_out, uint64_t n, b2co_stream s)
 {
     if (int st = check_table(t)) return st;
     if (n == 0 || !host_keys || !host_out) return B2CO_OK;
     uint32_t const kb = t->desc.key_bytes;
     uint32_t const ob = t->desc.value_bytes ? t->desc.value_bytes : kb;
-    uint64_t const chunk = 1ull << 24;  // keys per chunk
+    uint64_t const chunk = 1ull << 22;  // keys per chunk
     if (!t->stage) {
         t->stage_keys = chunk;
-        B2CO_CUDA(cudaMalloc(&t->stage, 2 * chunk * (kb + ob)));
+        B2CO_CUDA(cudaMalloc(&t->stage, kHostSlots * chunk * (kb + ob)));
         for (auto& p : t->pipe) B2CO_CUDA(cudaStreamCreateWithFlags(&p, cudaStreamNonBlocking));
         for (auto& e : t->ev) B2CO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     cudaStream_t c = cs(s);
-    B2CO_CUDA(cudaEventRecord(t->ev[2], c));
-    for (auto& p : t->pipe) B2CO_CUDA(cudaStreamWaitEvent(p, t->ev[2], 0));
+    B2CO_CUDA(cudaEventRecord(t->ev[kHostSlots], c));
+    for (auto& p : t->pipe) B2CO_CUDA(cudaStreamWaitEvent(p, t->ev[kHostSlots], 0));
     char* base = static_cast<char*>(t->stage);
     for (uint64_t off = 0, c_i = 0; off < n; off += chunk, ++c_i) {
         uint64_t m = n - off < chunk ? n - off : chunk;
-        int slot = int(c_i & 1);
+        int slot = int(c_i % kHostSlots);
         cudaStream_t p = t->pipe[slot];
         char* dk = base + uint64_t(slot) * chunk * (kb + ob);
         char* dout = dk + chunk * kb;
@@ -619,7 +625,7 @@ int b2co_oa_find_host(b2co_oa_table* t, void const* host_keys, void* host_out, u
         if (int st = launch_find(t, false, dk, nullptr, dout, m, p)) return st;
         B2CO_CUDA(cudaMemcpyAsync(static_cast<char*>(host_out) + off * ob, dout, m * ob, cudaMemcpyDeviceToHost, p));
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kHostSlots; ++i) {
         B2CO_CUDA(cudaEventRecord(t->ev[i], t->pipe[i]));
         B2CO_CUDA(cudaStreamWaitEvent(c, t->ev[i], 0));
     }
