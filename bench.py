@@ -408,9 +408,41 @@ def measure_e2e(t, q, out, stream, world, args):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), world) / e2e_steps
     assert torch.equal(ho, out.cpu()), "host-buffer Find differs from device Find"
+    floor_ms = pcie_floor_ms(hq, ho, q, out)
     return {"value": round(world * N_QUERIES / (e2e_ms / 1e3) / 1e9, 4), "unit": UNIT,
             "h2d_bytes_per_step": N_QUERIES * 8, "d2h_bytes_per_step": N_QUERIES * 8,
-            "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 22) - 1) >> 22}
+            "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 22) - 1) >> 22,
+            "pcie_floor_ms": round(floor_ms, 3), "frac_of_pcie_floor": round(floor_ms / e2e_ms, 4)}
+
+
+def pcie_floor_ms(hq, ho, q, out):
+    """Time of the step's bare copies alone: the keys in and the results out at
+    once on two streams, the same pinned buffers and byte counts as one e2e step.
+    No lookup can finish a step faster; measured after the timed e2e region."""
+    import torch
+    dq, dout = torch.empty_like(q), torch.empty_like(out)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def both():
+        cur = torch.cuda.current_stream()
+        s1.wait_stream(cur)
+        s2.wait_stream(cur)
+        with torch.cuda.stream(s1):
+            dq.copy_(hq, non_blocking=True)
+        with torch.cuda.stream(s2):
+            ho.copy_(dout, non_blocking=True)
+        cur.wait_stream(s1)
+        cur.wait_stream(s2)
+
+    both()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        both()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 5
 
 
 def window_gather_ceiling(t, stream, find_gkeys, windows_mean):
@@ -545,11 +577,76 @@ def extra_measurements(t, keys, q50, out, stream, args):
     ms = timed(lambda: t.FindAsync(q8, out))
     res["find_lf08_hit50_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
     del q8
+    res.update(small_map_measurements(stream))
     res.update(bloom_hll_measurements(stream))
     res.update(batched_measurements(stream))
     res.update(multi_measurements(stream))
     res.update(roaring_measurements(stream))
     res.update(served_measurements(stream))
+    return res
+
+
+def small_map_measurements(stream, reps=200):
+    """The small single-table workload: StaticMap<int32,int32>, DoubleHashing<xxhash_32>,
+    bucket 5, requested capacity 2,097,152 (2,621,735 slots, 21 MB: it stays in the
+    126 MB L2), 1,000,000 unique keys uniform in [0, 2^31-2] (seed 1), value 2*key+1,
+    1,000,000 queries at 50% hits (misses drawn from the same range and rejected
+    against the inserted set), shuffled.  L2-resident, so GB/s of algorithmic bytes
+    (4 key + 4 value + 40 per bucket window) is reported, not an HBM fraction.  Each
+    launch is short, so `reps` back-to-back launches are timed."""
+    import b2co
+    import torch
+    rng = np.random.default_rng(1)
+    n = 1_000_000
+    draw = np.unique(rng.integers(0, 2**31 - 1, size=int(n * 1.05), dtype=np.int64))
+    rng.shuffle(draw)
+    keys = draw[:n].astype(np.int32)
+    vals = (2 * keys.astype(np.int64) + 1).astype(np.int32)
+    cand = rng.integers(0, 2**31 - 1, size=n, dtype=np.int64).astype(np.int32)
+    miss = cand[~np.isin(cand, keys)][: n // 2]
+    q = np.concatenate([keys[rng.integers(0, n, size=n // 2)], miss])
+    rng.shuffle(q)
+    exp = np.where(np.isin(q, keys), (2 * q.astype(np.int64) + 1).astype(np.int32), np.int32(-1))
+    t = b2co.StaticMap(2_097_152, -1, -1, key_dtype=torch.int32, value_dtype=torch.int32)
+    dk, dv, dq = (torch.from_numpy(a).cuda() for a in (keys, vals, q))
+    pairs = b2co.pack_pairs(dk, dv)
+    out = torch.empty(len(q), dtype=torch.int32, device="cuda")
+    flags = torch.empty(len(q), dtype=torch.uint8, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    insert_ms = 0.0
+    for i in range(reps // 10 + 3):
+        ev[0].record(stream)
+        t.ClearAsync(stream=stream)
+        ev[1].record(stream)
+        t.InsertAsync(pairs, stream=stream)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        if i >= 3:
+            insert_ms += ev[1].elapsed_time(ev[2])
+    insert_ms /= reps // 10
+
+    def timed(fn):
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        for _ in range(reps):
+            fn()
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / reps
+
+    find_ms = timed(lambda: t.FindAsync(dq, out, stream=stream))
+    ok = bool(np.array_equal(out.cpu().numpy(), exp))
+    contains_ms = timed(lambda: t.ContainsAsync(dq, flags, stream=stream))
+    ok = ok and bool(np.array_equal(flags.cpu().numpy(), (exp != -1).astype(np.uint8)))
+    res = {"small_map_capacity": t.Capacity(), "small_map_insert_gkeys": round(n / insert_ms / 1e6, 3),
+           "small_map_find_gkeys": round(len(q) / find_ms / 1e6, 3),
+           "small_map_find_gbs_1window": round(len(q) * 48 / find_ms / 1e6, 1),
+           "small_map_contains_gkeys": round(len(q) / contains_ms / 1e6, 3),
+           "small_map_find_us_per_launch": round(find_ms * 1e3, 2), "small_map_results_exact": ok}
+    del t
     return res
 
 
@@ -1045,7 +1142,8 @@ def main():
     ap.add_argument("--sweep", action="store_true", help="time every Find kernel shape and report each")
     ap.add_argument("--sweep-shapes", default="", help="comma-separated shapes for --sweep (default: a fixed list)")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
-    ap.add_argument("--only", default="", choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring"],
+    ap.add_argument("--only", default="",
+                    choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring", "small_map"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
     ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
     args = ap.parse_args()
@@ -1057,7 +1155,8 @@ def main():
         import torch
         fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,
               "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2),
-              "multi": multi_measurements, "roaring": roaring_measurements}[args.only]
+              "multi": multi_measurements, "roaring": roaring_measurements,
+              "small_map": small_map_measurements}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
         run_reference(args)
