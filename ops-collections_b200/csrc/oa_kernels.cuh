@@ -11,9 +11,12 @@
 //    so the key and payload appear together and no reader ever waits for a
 //    payload (the reference's unbounded WaitForPayload spin does not exist);
 //  * lookups read the table through the non-coherent path with 16-byte vector
-//    loads, either one lane per key (all B slots of the window issued back to
-//    back, several keys per lane in flight) or G lanes per key (one slot per
-//    lane, the window resolved with warp ballots);
+//    loads and a 64-byte L2 fill hint.  The default lookup (k_find_wdefer)
+//    stages keys per warp with bulk copies, gives each bucket window G lanes
+//    (one slot per lane and round, the tile agreeing on the first stopping
+//    slot by a min over shuffles), and queues the rare keys that need further
+//    windows so each pass waits on one window load; one-lane-per-key and
+//    ballot-resolved shapes remain selectable;
 //  * every loop is bounded by the probe cycle, so no kernel can spin.
 #pragma once
 
