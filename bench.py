@@ -586,6 +586,53 @@ def extra_measurements(t, keys, q50, out, stream, args):
     return res
 
 
+def insert_measurements(stream, capacity_log2=28, reps=3):
+    """The write side of the headline table on its own: StaticMap<int64,int64>,
+    DoubleHashing<xxhash_32>, bucket 5, requested capacity 2^capacity_log2; a
+    cleared table filled to LF 0.5 by Insert (unique keys), by InsertAndFind in
+    race and in first-wins mode, then every pair upserted again by
+    InsertOrAssign (all duplicates: payload overwrites).  Clears are not timed;
+    each figure is the best of `reps`.  The insert stream of first-wins is
+    checked: every key inserted once, every found payload its own."""
+    import b2co
+    import torch
+    t = b2co.StaticMap(1 << capacity_log2, -1, -1, key_dtype=torch.int64, value_dtype=torch.int64, bucket_size=5,
+                       probing=b2co.PROBE_DOUBLE, hash_kind=b2co.HASH_XXH32)
+    unique, _ = workload_sizes(t.Capacity(), LOAD_FACTOR)
+    keys = mix64_torch(counters(KEY_STREAM, unique, "torch"))
+    vals = mix64_torch(counters(VALUE_STREAM, unique, "torch"))
+    pairs = b2co.pack_pairs(keys, vals)
+    found = torch.empty(unique, dtype=torch.int64, device="cuda")
+    ins = torch.empty(unique, dtype=torch.uint8, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def best(fn, clear=True):
+        out = []
+        for _ in range(reps):
+            if clear:
+                t.ClearAsync(stream=stream)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return min(out)
+
+    res = {"insert_capacity": t.Capacity(), "insert_pairs": unique}
+    ms = best(lambda: t.InsertAsync(pairs, stream=stream))
+    res["insert_gkeys"] = round(unique / ms / 1e6, 3)
+    ms = best(lambda: t.InsertAndFindAsync(pairs, found, ins, stream=stream, mode=b2co.IAF_RACE))
+    res["insert_and_find_race_gkeys"] = round(unique / ms / 1e6, 3)
+    ms = best(lambda: t.InsertAndFindAsync(pairs, found, ins, stream=stream, mode=b2co.IAF_FIRST_WINS))
+    res["insert_and_find_first_wins_gkeys"] = round(unique / ms / 1e6, 3)
+    res["first_wins_exact"] = bool(int(ins.sum().item()) == unique) and bool(torch.equal(found, vals))
+    ms = best(lambda: t.InsertOrAssignAsync(pairs, stream=stream), clear=False)
+    res["insert_or_assign_dup_gkeys"] = round(unique / ms / 1e6, 3)
+    del t
+    return res
+
+
 def small_map_measurements(stream, reps=200):
     """The small single-table workload: StaticMap<int32,int32>, DoubleHashing<xxhash_32>,
     bucket 5, requested capacity 2,097,152 (2,621,735 slots, 21 MB: it stays in the
@@ -1143,7 +1190,8 @@ def main():
     ap.add_argument("--sweep-shapes", default="", help="comma-separated shapes for --sweep (default: a fixed list)")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
     ap.add_argument("--only", default="",
-                    choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring", "small_map"],
+                    choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring", "small_map",
+                             "insert"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
     ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
     args = ap.parse_args()
@@ -1156,7 +1204,8 @@ def main():
         fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,
               "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2),
               "multi": multi_measurements, "roaring": roaring_measurements,
-              "small_map": small_map_measurements}[args.only]
+              "small_map": small_map_measurements,
+              "insert": lambda st: insert_measurements(st, capacity_log2=args.capacity_log2)}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
         run_reference(args)
