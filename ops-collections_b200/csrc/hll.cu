@@ -79,16 +79,20 @@ __global__ void __launch_bounds__(512) k_hll_add_shared(uint32_t* regs, uint32_t
     __syncthreads();
     uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
     uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    // two keys per iteration keep two independent hash chains in flight
-    for (; i + stride < n; i += 2 * stride) {
-        uint64_t k0 = load_key<KB>(keys, i), k1 = load_key<KB>(keys, i + stride);
-        uint32_t x0, r0, x1, r1;
-        hll_locate<KB>(k0, p, x0, r0);
-        hll_locate<KB>(k1, p, x1, r1);
-        raise_register(sk, x0, r0);
-        raise_register(sk, x1, r1);
+    // kItems keys per iteration keep as many independent load-and-hash chains in
+    // flight (the sketch's shared memory, not registers, limits the CTAs per SM)
+    constexpr int kItems = 4;
+    for (; i + (kItems - 1) * stride < n; i += kItems * stride) {
+        uint64_t k[kItems];
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) k[j] = load_key<KB>(keys, i + j * stride);
+        uint32_t x[kItems], r[kItems];
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) hll_locate<KB>(k[j], p, x[j], r[j]);
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) raise_register(sk, x[j], r[j]);
     }
-    if (i < n) {
+    for (; i < n; i += stride) {
         uint32_t x, r;
         hll_locate<KB>(load_key<KB>(keys, i), p, x, r);
         raise_register(sk, x, r);
