@@ -580,6 +580,7 @@ def extra_measurements(t, keys, q50, out, stream, args):
     res["find_lf08_hit50_gkeys"] = round(N_QUERIES / ms / 1e6, 3)
     del q8
     res.update(small_map_measurements(stream))
+    res.update(dynamic_map_measurements(stream))
     res.update(bloom_hll_measurements(stream))
     res.update(batched_measurements(stream))
     res.update(multi_measurements(stream))
@@ -632,6 +633,58 @@ def insert_measurements(stream, capacity_log2=28, reps=3):
     ms = best(lambda: t.InsertOrAssignAsync(pairs, stream=stream), clear=False)
     res["insert_or_assign_dup_gkeys"] = round(unique / ms / 1e6, 3)
     del t
+    return res
+
+
+def dynamic_map_measurements(stream, log2n=26, batch_log2=22):
+    """DynamicMap<int64,int64> (the reference's defaults: LinearProbing<murmurhash3_32>,
+    bucket 5): created for 2^20 slots, then 2^log2n unique pairs inserted in
+    batches of 2^batch_log2 -- the map adds a submap of twice the capacity
+    whenever the load would pass 0.6, so the timed inserts include every growth
+    step -- and Find / Contains of 2^log2n queries at 50% hits over all the
+    submaps.  Hits must return their own values, misses the empty value."""
+    import b2co
+    import torch
+    n, bs = 1 << log2n, 1 << batch_log2
+    keys = mix64_torch(counters(11 << 40, n, "torch")) >> 1
+    vals = mix64_torch(counters(12 << 40, n, "torch")) >> 1
+    g = torch.Generator(device="cuda").manual_seed(SEED + 31)
+    hit = torch.rand(n, generator=g, device="cuda") < 0.5
+    pick = torch.randint(0, n, (n,), generator=g, device="cuda")
+    q = torch.where(hit, keys[pick], mix64_torch(counters(13 << 40, n, "torch")) >> 1)
+    exp = torch.where(hit, vals[pick], torch.full_like(vals, -1))
+    pairs = b2co.pack_pairs(keys, vals)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m = b2co.DynamicMap(1 << 20, -1, -1, -2, key_dtype=torch.int64, value_dtype=torch.int64)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    inserted = 0
+    for off in range(0, n, bs):
+        inserted += m.Insert(pairs[off:off + bs], stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    insert_ms = e0.elapsed_time(e1)
+    out = torch.empty(n, dtype=torch.int64, device="cuda")
+    m.Find(q, out, stream=stream)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    m.Find(q, out, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    find_ms = e0.elapsed_time(e1)
+    exact = bool(torch.equal(out, exp))
+    flags = torch.empty(n, dtype=torch.uint8, device="cuda")
+    e0.record(stream)
+    m.Contains(q, flags, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    contains_ms = e0.elapsed_time(e1)
+    exact = exact and bool(torch.equal(flags.bool(), hit))
+    res = {"dmap_pairs": n, "dmap_inserted": inserted, "dmap_submaps": m.NumSubmaps(), "dmap_capacity": m.Capacity(),
+           "dmap_insert_with_growth_gkeys": round(n / insert_ms / 1e6, 3),
+           "dmap_find_gkeys": round(n / find_ms / 1e6, 3), "dmap_contains_gkeys": round(n / contains_ms / 1e6, 3),
+           "dmap_results_exact": exact}
+    del m
     return res
 
 
@@ -1193,7 +1246,7 @@ def main():
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
     ap.add_argument("--only", default="",
                     choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring", "small_map",
-                             "insert"],
+                             "insert", "dmap"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
     ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
     args = ap.parse_args()
@@ -1206,7 +1259,7 @@ def main():
         fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,
               "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2),
               "multi": multi_measurements, "roaring": roaring_measurements,
-              "small_map": small_map_measurements,
+              "small_map": small_map_measurements, "dmap": dynamic_map_measurements,
               "insert": lambda st: insert_measurements(st, capacity_log2=args.capacity_log2)}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
