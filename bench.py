@@ -763,12 +763,13 @@ def mix32_torch(x):
     return x ^ (x >> 16)
 
 
-def batched_measurements(stream):
-    """Batched tables: 4,096 StaticMap<int32,int32> (DoubleHashing<xxhash_32>, bucket 5)
-    at load factor 0.5 with log-normal key counts (median 32,768, sigma(log2) = 2.0,
-    clipped to [1,024; 4,194,304]); each table inserts its own keys, then finds 2x its
-    key count at 50% hits.  One persistent group launch (and its CUDA-graph replay,
-    lane count from the autotuner) against one plain launch per table."""
+def batched_workload():
+    """The batched workload's inputs, on the device: 4,096 StaticMap<int32,int32>
+    tables with log-normal key counts (median 32,768, sigma(log2) = 2.0, clipped
+    to [1,024; 4,194,304]); per table its own distinct keys, then 2x its key
+    count of queries at 50% hits.  Returns the per-table sizes and offsets
+    (numpy) and the concatenated keys, values, packed pairs, queries and the
+    hit mask (tensors)."""
     import torch
     import b2co
     rng = np.random.default_rng(SEED + 11)
@@ -787,7 +788,8 @@ def batched_measurements(stream):
     keys = k32.to(torch.int32)  # two's-complement wrap of the uint32 value
     vals = (k32 >> 1).to(torch.int32)  # never the -1 sentinel
     pairs = b2co.pack_pairs(keys, vals)
-    del t_of, j, salt, k32, vals
+    vals_keep = vals
+    del t_of, j, salt, k32
     g = torch.Generator(device="cuda").manual_seed(SEED + 12)
     qt = torch.repeat_interleave(torch.arange(count, device="cuda"), 2 * torch.from_numpy(sizes).cuda())
     qj = torch.arange(2 * total, device="cuda") - torch.from_numpy(q_off[:-1]).cuda()[qt]
@@ -800,6 +802,22 @@ def batched_measurements(stream):
     miss = mix32_torch((qj + (1 << 30)) ^ qsalt).to(torch.int64).to(torch.int32)  # j >= 2^30 never used above
     q = torch.where(hit, hit_keys, miss)
     del qt, qj, n_t, base, rnd, hit_keys, qsalt, miss
+    return {"count": count, "sizes": sizes, "total": total, "ins_off": ins_off, "q_off": q_off, "keys": keys,
+            "vals": vals_keep, "pairs": pairs, "queries": q, "hit": hit}
+
+
+def batched_measurements(stream):
+    """Batched tables: 4,096 StaticMap<int32,int32> (DoubleHashing<xxhash_32>, bucket 5)
+    at load factor 0.5 with log-normal key counts (median 32,768, sigma(log2) = 2.0,
+    clipped to [1,024; 4,194,304]); each table inserts its own keys, then finds 2x its
+    key count at 50% hits.  One persistent group launch (and its CUDA-graph replay,
+    lane count from the autotuner) against one plain launch per table."""
+    import torch
+    import b2co
+    w = batched_workload()
+    count, sizes, total, ins_off, q_off = w["count"], w["sizes"], w["total"], w["ins_off"], w["q_off"]
+    pairs, q, hit = w["pairs"], w["queries"], w["hit"]
+    del w
     d_ins_off = torch.from_numpy(ins_off).cuda()
     d_q_off = torch.from_numpy(q_off).cuda()
     out = torch.empty(2 * total, dtype=torch.int32, device="cuda")
@@ -870,8 +888,7 @@ def bloom_hll_measurements(stream, bloom=True, hll_log2=30):
     if bloom:
         res.update(bloom_part(f_time=time_once, g=g, peak=peak))
     n_hll = 1 << hll_log2
-    distinct = mix64_torch(counters(5 << 40, 10_000_000, "torch"))
-    keys = distinct[torch.randint(0, distinct.numel(), (n_hll,), generator=g, device="cuda")]
+    keys = hll_keys(g, n_hll)
     h = b2co.HyperLogLog(16)
     h.AddAsync(keys[: 1 << 20])
     h.Clear()
@@ -894,16 +911,34 @@ def bloom_hll_measurements(stream, bloom=True, hll_log2=30):
     return res
 
 
+def bloom_workload(g):
+    """A filter of 2^22 blocks (2^30 bits), 2^28 uniform 64-bit adds, and 2^28
+    queries: half drawn from the adds, half from a disjoint stream, in that
+    order.  Returns (num_blocks, adds, queries) on the device."""
+    import torch
+    nb, n = 1 << 22, 1 << 28
+    adds = mix64_torch(counters(3 << 40, n, "torch"))
+    absent = mix64_torch(counters(4 << 40, n // 2, "torch"))
+    q = torch.cat([adds[torch.randint(0, n, (n // 2,), generator=g, device="cuda")], absent])
+    return nb, adds, q
+
+
+def hll_keys(g, n):
+    """n int64 HyperLogLog inputs drawn uniformly with replacement from 10^7
+    distinct uniform keys, on the device."""
+    import torch
+    distinct = mix64_torch(counters(5 << 40, 10_000_000, "torch"))
+    return distinct[torch.randint(0, distinct.numel(), (n,), generator=g, device="cuda")]
+
+
 def bloom_part(f_time, g, peak):
     import torch
     import b2co
     res = {}
     time_once = f_time
-    nb, n = 1 << 22, 1 << 28
+    nb, adds, q = bloom_workload(g)
+    n = adds.numel()
     f = b2co.BloomFilter(nb, key_dtype=torch.int64)
-    adds = mix64_torch(counters(3 << 40, n, "torch"))
-    absent = mix64_torch(counters(4 << 40, n // 2, "torch"))
-    q = torch.cat([adds[torch.randint(0, n, (n // 2,), generator=g, device="cuda")], absent])
     f.AddAsync(adds)  # warm-up: the same batch, so the timed Add runs the path (and scratch) it will use
     f.Clear()
     ms = time_once(lambda: f.AddAsync(adds))

@@ -79,19 +79,41 @@ int b2co_set_l2_fetch_granularity(uint32_t bytes, uint64_t* applied);
 /* Open-addressing tables: StaticMap<K,T> and StaticSet<K>                 */
 /* ===================================================================== */
 
+/* How keys compare (KeyEqual): the reference's default EqualTo is ==
+ * (utility/math_utils.h:66-70, applied by utility/equal_wrapper.h:30-33).  For
+ * integer keys that is bit equality; for floating-point keys it is IEEE
+ * equality, so -0.0 matches +0.0 and a NaN matches nothing.  Empty and erased
+ * sentinels are always compared bitwise (equal_wrapper.h:35-42,
+ * utility/traits.h:27-28), and hashes read the key's bytes, so -0.0 and +0.0
+ * start different probe sequences exactly as in the reference. */
+typedef enum {
+    B2CO_KEY_INTEGER = 0, /* integer keys of 2, 4 or 8 bytes (int16/uint16/int32/uint32/int64/uint64) */
+    B2CO_KEY_FLOAT = 1    /* fp16 (2 bytes), float (4) or double (8) keys */
+} b2co_key_kind;
+
 typedef struct {
-    uint32_t key_bytes;        /* 4 or 8 */
-    uint32_t value_bytes;      /* 0 = StaticSet, else 4 or 8 */
+    uint32_t key_bytes;        /* 2, 4 or 8 */
+    uint32_t value_bytes;      /* 0 = StaticSet, else 2, 4 or 8 (2 only with 2-byte keys) */
     uint32_t bucket_size;      /* Storage<B>: 1, 2, 4, 5 or 8 */
     uint32_t probing;          /* b2co_probing */
-    uint32_t hash;             /* b2co_hash used by the probing scheme */
-    uint32_t reserved;         /* must be 0 */
+    uint32_t hash;             /* b2co_hash used by the probing scheme (Fmix: 4- or 8-byte keys) */
+    uint32_t key_kind;         /* b2co_key_kind (0 = integer keys) */
     uint64_t empty_key_bits;   /* sentinel bit patterns (low key_bytes / value_bytes bytes) */
     uint64_t empty_value_bits;
     uint64_t erased_key_bits;  /* tombstone key; equal to empty_key_bits = no tombstone */
 } b2co_oa_desc;
 
 typedef struct b2co_oa_table b2co_oa_table;
+
+/* The kernels' key primitives evaluated on the host (the same source as the
+ * device code), so callers and tests can check them without a GPU.
+ * b2co_probe_hash: the 32-bit probe hash of a key's bytes.
+ * reference: detail/hash_functions/xxhash.h:52-326, murmurhash3.h:20-106,
+ * utils.h:42-66, utility/math_utils.h:14-24 (SanitizeHash).
+ * b2co_key_equal: the key comparison of a table of that key kind.
+ * reference: utility/equal_wrapper.h:30-33, utility/math_utils.h:66-70. */
+int b2co_probe_hash(uint32_t hash, uint32_t key_bytes, uint64_t key_bits, uint32_t seed, uint32_t* out);
+int b2co_key_equal(uint32_t key_kind, uint32_t key_bytes, uint64_t a_bits, uint64_t b_bits, int* equal);
 
 /* Capacity the table gets for a requested slot count.
  * reference: include/detail/extent/extent.inl:20-62 (MakeValidExtent). */
@@ -160,10 +182,11 @@ int b2co_oa_insert_and_find_async(b2co_oa_table* table, const void* pairs, void*
  * and synchronous like it, but the scratch (4 bytes per item, 4 + 1/8 bytes
  * per table slot) comes from a fixed 32 MiB device array inside the library,
  * which every GPU that loads the library holds until the process exits.
- * Batches needing more scratch fail with B2CO_ERANGE.  The first call on a
- * device looks up the array's address there; make that call before any stream
- * capture begins.  All calls share the array, so calls that overlap on the GPU
- * race: serialize them. */
+ * Batches needing more scratch fail with B2CO_ERANGE.  Every call looks up
+ * the array's address on the current device; the first call on a device also
+ * loads the array there, so make that call before any stream capture begins.
+ * All calls share the array, so calls that overlap on the GPU race: serialize
+ * them. */
 int b2co_oa_insert_and_find_noalloc(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
                                     uint64_t n, b2co_stream stream);
 /* Erase (returns the count of keys not erased).
@@ -214,6 +237,15 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
  * does not settle them are queued and followed a whole pass at a time. */
 #define B2CO_FIND_DEFERRED 0x800u
 int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_lane);
+/* Kernel shape of the insert family (Insert, InsertIf, InsertOrAssign,
+ * InsertAndFind) for this table (no reference counterpart; results do not
+ * depend on it).  lanes_per_key 1 runs one lane per key (the reference's scan
+ * as written); 2, 4 or 8 lanes share each bucket window with keys_per_tile
+ * (1, 2 or 4) keys in flight per lane group.  (0, 0) restores the default:
+ * 4 lanes, 2 keys (one lane per key for bucket size 1).  Layouts with 2-byte
+ * or floating-point keys run the default window shape for any request other
+ * than one lane per key. */
+int b2co_oa_set_write_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_tile);
 
 /* ===================================================================== */
 /* Table groups: many independent tables, one launch per operation          */

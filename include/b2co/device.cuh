@@ -20,31 +20,37 @@
 namespace b2co {
 
 // ---------------------------------------------------------------------------
-// hashes over a key's object representation (little-endian, 4 or 8 bytes)
+// hashes over a key's object representation (little-endian, 2, 4 or 8 bytes)
 // ---------------------------------------------------------------------------
 
 B2CO_HD uint32_t rotl32(uint32_t x, int r) { return (x << r) | (x >> (32 - r)); }
 B2CO_HD uint64_t rotl64(uint64_t x, int r) { return (x << r) | (x >> (64 - r)); }
 
-// XXH32 for 4- and 8-byte inputs (include/detail/hash_functions/xxhash.h:52-175:
-// inputs shorter than 16 bytes take the seed+prime5 start and 4-byte lanes).
+// XXH32 for 2-, 4- and 8-byte inputs (include/detail/hash_functions/xxhash.h:52-175:
+// inputs shorter than 16 bytes take the seed+prime5 start, then 4-byte lanes,
+// then single bytes).
 template <int KB>
 B2CO_HD uint32_t xxh32(uint64_t key, uint32_t seed)
 {
     constexpr uint32_t P1 = 0x9e3779b1u, P2 = 0x85ebca77u, P3 = 0xc2b2ae3du, P4 = 0x27d4eb2fu, P5 = 0x165667b1u;
     uint32_t h = seed + P5 + uint32_t(KB);
-    h = rotl32(h + uint32_t(key) * P3, 17) * P4;
-    if constexpr (KB == 8) h = rotl32(h + uint32_t(key >> 32) * P3, 17) * P4;
+    if constexpr (KB == 2) {
+        h = rotl32(h + uint32_t(key & 0xffu) * P5, 11) * P1;
+        h = rotl32(h + uint32_t((key >> 8) & 0xffu) * P5, 11) * P1;
+    } else {
+        h = rotl32(h + uint32_t(key) * P3, 17) * P4;
+        if constexpr (KB == 8) h = rotl32(h + uint32_t(key >> 32) * P3, 17) * P4;
+    }
     h ^= h >> 15;
     h *= P2;
     h ^= h >> 13;
     h *= P3;
     h ^= h >> 16;
-    (void)P1;
     return h;
 }
 
-// XXH64 for 4- and 8-byte inputs (xxhash.h:184-326, fast paths :199-218).
+// XXH64 for 2-, 4- and 8-byte inputs (xxhash.h:184-326, fast paths :199-218,
+// single trailing bytes after them).
 template <int KB>
 B2CO_HD uint64_t xxh64(uint64_t key, uint64_t seed)
 {
@@ -54,6 +60,11 @@ B2CO_HD uint64_t xxh64(uint64_t key, uint64_t seed)
     if constexpr (KB == 8) {
         h ^= rotl64(key * P2, 31) * P1;
         h = rotl64(h, 27) * P1 + P4;
+    } else if constexpr (KB == 2) {
+        h ^= uint64_t(key & 0xffu) * P5;
+        h = rotl64(h, 11) * P1;
+        h ^= uint64_t((key >> 8) & 0xffu) * P5;
+        h = rotl64(h, 11) * P1;
     } else {
         h ^= uint64_t(uint32_t(key)) * P1;
         h = rotl64(h, 23) * P2 + P3;
@@ -88,7 +99,7 @@ B2CO_HD uint64_t fmix64(uint64_t k, uint64_t seed)
     return h;
 }
 
-// MurmurHash3_x86_32 for 4- and 8-byte inputs (hash_functions/murmurhash3.h:57-106).
+// MurmurHash3_x86_32 for 2-, 4- and 8-byte inputs (hash_functions/murmurhash3.h:57-106).
 template <int KB>
 B2CO_HD uint32_t murmur3_32(uint64_t key, uint32_t seed)
 {
@@ -104,12 +115,21 @@ B2CO_HD uint32_t murmur3_32(uint64_t key, uint32_t seed)
         h = rotl32(h, 13);
         h = h * 5 + 0xe6546b64u;
     }
+    if constexpr (KB == 2) {  // the two tail bytes
+        uint32_t k = uint32_t(key & 0xffffu);
+        k *= c1;
+        k = rotl32(k, 15);
+        k *= c2;
+        h ^= k;
+    }
     h ^= uint32_t(KB);
     return fmix32(h, 0);
 }
 
 // The probing schemes cast the hash to the kernels' uint32 size type
-// (utility/math_utils.h:14-24 SanitizeHash).
+// (utility/math_utils.h:14-24 SanitizeHash).  The Fmix family takes 4- and
+// 8-byte keys only (utils.h:42-66 static_asserts the size); tables refuse it
+// for other widths.
 template <int KB>
 B2CO_HD uint32_t probe_hash(uint32_t kind, uint64_t key, uint32_t seed)
 {
@@ -117,7 +137,8 @@ B2CO_HD uint32_t probe_hash(uint32_t kind, uint64_t key, uint32_t seed)
         case B2CO_HASH_MURMUR3_32: return murmur3_32<KB>(key, seed);
         case B2CO_HASH_FMIX:
             if constexpr (KB == 4) return fmix32(uint32_t(key), seed);
-            else return uint32_t(fmix64(key, seed));
+            else if constexpr (KB == 8) return uint32_t(fmix64(key, seed));
+            else return 0;
         case B2CO_HASH_XXH64: return uint32_t(xxh64<KB>(key, seed));
         default: return xxh32<KB>(key, seed);
     }
@@ -202,18 +223,45 @@ struct alignas(16) U128 {
     uint64_t lo, hi;
 };
 
-template <int KB, int VB>
+// Key equality (KeyEqual = EqualTo, utility/math_utils.h:66-70, applied by
+// equal_wrapper.h:30-33).  Integer keys compare their bits.  Floating-point
+// keys (fp16, fp32, fp64 by width) compare as IEEE values: -0 equals +0 and a
+// NaN equals nothing, itself included.  Sentinel tests stay bitwise
+// (equal_wrapper.h:35-42 with traits.h:27-28), so they never call this.
+template <int KB, bool FLOAT_KEY>
+B2CO_HD bool key_equal(uint64_t a, uint64_t b)
+{
+    if constexpr (!FLOAT_KEY) {
+        return a == b;
+    } else {
+        constexpr uint64_t sign = 1ull << (8 * KB - 1);
+        constexpr uint64_t inf = KB == 2 ? 0x7c00ull : (KB == 4 ? 0x7f800000ull : 0x7ff0000000000000ull);
+        uint64_t const ma = a & ~sign, mb = b & ~sign;  // magnitudes (keys arrive masked to KB bytes)
+        if (ma > inf || mb > inf) return false;         // a NaN on either side
+        return a == b || (ma | mb) == 0;                 // same value, or +0 against -0
+    }
+}
+
+// A slot: Pair<K,V> aligned to min(16, bitceil(sizeof K + sizeof V)) with the
+// payload at the next offset aligned to its own size, or a bare key for sets.
+// FLOAT_KEY selects IEEE key equality (fp16/fp32/fp64 keys by width).
+template <int KB, int VB, bool FLOAT_KEY = false>
 struct SlotT {
     static constexpr int key_bytes = KB;
     static constexpr int value_bytes = VB;
     static constexpr bool is_set = VB == 0;
+    static constexpr bool float_key = FLOAT_KEY;
     static constexpr int value_offset = VB == 0 ? 0 : ((KB + VB - 1) / VB) * VB;
-    static constexpr int bytes = VB == 0 ? KB : ((value_offset + VB) <= 8 ? 8 : 16);
+    static constexpr int pair_align = (KB + VB) <= 4 ? 4 : ((KB + VB) <= 8 ? 8 : 16);
+    static constexpr int bytes = VB == 0 ? KB : ((value_offset + VB + pair_align - 1) / pair_align) * pair_align;
     // raw storage word of one slot
-    using Raw = typename std::conditional<bytes == 4, uint32_t,
-                typename std::conditional<bytes == 8, unsigned long long, U128>::type>::type;
-    static constexpr uint64_t kmask = KB == 8 ? ~0ull : 0xffffffffull;
-    static constexpr uint64_t vmask = VB == 8 ? ~0ull : (VB == 4 ? 0xffffffffull : 0ull);
+    using Raw = typename std::conditional<bytes == 2, unsigned short,
+                typename std::conditional<bytes == 4, uint32_t,
+                typename std::conditional<bytes == 8, unsigned long long, U128>::type>::type>::type;
+    static constexpr uint64_t kmask = KB == 8 ? ~0ull : ((1ull << (8 * KB)) - 1ull);
+    static constexpr uint64_t vmask = VB == 8 ? ~0ull : (VB == 0 ? 0ull : ((1ull << (8 * VB)) - 1ull));
+
+    B2CO_HD static bool key_eq(uint64_t a, uint64_t b) { return key_equal<KB, FLOAT_KEY>(a, b); }
 
     B2CO_HD static uint64_t key(Raw r)
     {
@@ -224,9 +272,8 @@ struct SlotT {
     B2CO_HD static uint64_t value(Raw r)
     {
         if constexpr (is_set) return key(r);
-        else if constexpr (bytes == 8) return uint64_t(r) >> 32;
-        else if constexpr (value_offset == 8) return r.hi & vmask;
-        else return r.lo >> 32;  // unreachable for supported layouts
+        else if constexpr (bytes == 16) return r.hi & vmask;  // 16-byte pairs keep the payload at offset 8
+        else return (uint64_t(r) >> (8 * value_offset)) & vmask;
     }
     B2CO_HD static Raw make(uint64_t k, uint64_t v)
     {
@@ -235,11 +282,10 @@ struct SlotT {
             r.lo = k & kmask;
             r.hi = v & vmask;
             return r;
-        } else if constexpr (bytes == 8) {
-            if constexpr (is_set) return (unsigned long long)k;
-            else return (unsigned long long)((k & 0xffffffffull) | (v << 32));
+        } else if constexpr (is_set) {
+            return Raw(k & kmask);
         } else {
-            return uint32_t(k);
+            return Raw((k & kmask) | ((v & vmask) << (8 * value_offset)));
         }
     }
     // Same slot with the key replaced, every other byte kept.
@@ -248,14 +294,15 @@ struct SlotT {
         if constexpr (bytes == 16) {
             r.lo = (r.lo & ~kmask) | (k & kmask);
             return r;
-        } else if constexpr (bytes == 8 && !is_set) {
-            return (unsigned long long)((uint64_t(r) & ~0xffffffffull) | (k & 0xffffffffull));
+        } else if constexpr (!is_set) {
+            return Raw((uint64_t(r) & ~kmask) | (k & kmask));
         } else {
-            return Raw(k);
+            return Raw(k & kmask);
         }
     }
 };
 
+B2CO_HD bool raw_eq(unsigned short a, unsigned short b) { return a == b; }
 B2CO_HD bool raw_eq(uint32_t a, uint32_t b) { return a == b; }
 B2CO_HD bool raw_eq(unsigned long long a, unsigned long long b) { return a == b; }
 B2CO_HD bool raw_eq(U128 a, U128 b) { return a.lo == b.lo && a.hi == b.hi; }

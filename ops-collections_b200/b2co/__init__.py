@@ -23,7 +23,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libb2co.so")
+# B2CO_LIB names another build of the same library (e.g. one compiled with other tuning macros).
+LIB_PATH = os.environ.get("B2CO_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libb2co.so")
 
 OK, EINVAL, ERANGE, ENOMEM, ECUDA, ETIMEOUT, ELOGIC, EOVERFLOW = range(8)
 HASH_XXH32, HASH_MURMUR3_32, HASH_FMIX, HASH_XXH64 = range(4)
@@ -74,7 +75,7 @@ _EXC = {EINVAL: InvalidArgument, ERANGE: LengthError, ENOMEM: BadAlloc, ECUDA: C
 
 class OaDesc(C.Structure):
     _fields_ = [("key_bytes", C.c_uint32), ("value_bytes", C.c_uint32), ("bucket_size", C.c_uint32),
-                ("probing", C.c_uint32), ("hash", C.c_uint32), ("reserved", C.c_uint32),
+                ("probing", C.c_uint32), ("hash", C.c_uint32), ("key_kind", C.c_uint32),
                 ("empty_key_bits", C.c_uint64), ("empty_value_bits", C.c_uint64),
                 ("erased_key_bits", C.c_uint64)]
 
@@ -124,17 +125,32 @@ def _stream(stream):
     return C.c_void_p(stream.cuda_stream)
 
 
-def _bits(x, nbytes: int) -> int:
-    if isinstance(x, float):
-        fmt = {4: np.float32, 8: np.float64}[nbytes]
-        return int(np.array([x], dtype=fmt).view({4: np.uint32, 8: np.uint64}[nbytes])[0])
+KEY_INTEGER, KEY_FLOAT = 0, 1
+_FLOATS = {2: np.float16, 4: np.float32, 8: np.float64}
+_UINTS = {2: np.uint16, 4: np.uint32, 8: np.uint64}
+
+
+def _bits(x, nbytes: int, floating: bool = False) -> int:
+    """Bit pattern of a sentinel: the IEEE encoding of that width for a float
+    (or for any value when `floating`), two's complement for an integer."""
+    if floating or isinstance(x, (float, np.floating)):
+        return int(np.array([x], dtype=_FLOATS[nbytes]).view(_UINTS[nbytes])[0])
     return int(x) & ((1 << (8 * nbytes)) - 1)
 
 
+def _is_float(dt) -> bool:
+    return dt is not None and dt.is_floating_point
+
+
 def slot_bytes(key_bytes: int, value_bytes: int) -> int:
+    """Pair<K,V> aligned to min(16, bitceil(sizeof K + sizeof V)), payload at the
+    next offset aligned to its own size (pair.inl:19-24); a set slot is the key."""
     if value_bytes == 0:
         return key_bytes
-    return 8 if key_bytes + value_bytes == 8 else 16
+    s = key_bytes + value_bytes
+    align = 4 if s <= 4 else (8 if s <= 8 else 16)
+    end = (key_bytes + value_bytes - 1) // value_bytes * value_bytes + value_bytes
+    return (end + align - 1) // align * align
 
 
 def pack_pairs(keys, values):
@@ -144,6 +160,8 @@ def pack_pairs(keys, values):
     n = keys.numel()
     if kb == 4 and vb == 4:
         return torch.stack([keys.view(torch.int32), values.view(torch.int32)], dim=1).contiguous()
+    if kb == 2 and vb == 2:
+        return torch.stack([keys.view(torch.int16), values.view(torch.int16)], dim=1).contiguous()
     out = torch.zeros((n, 2), dtype=torch.int64, device=keys.device)
     if kb == 8:
         out[:, 0] = keys.view(torch.int64)
@@ -154,6 +172,12 @@ def pack_pairs(keys, values):
     else:
         out[:, 1] = values.view(torch.int32).to(torch.int64) & 0xFFFFFFFF
     return out
+
+
+def _int_view(t):
+    """The tensor's bits as a signed integer tensor of the same width."""
+    import torch
+    return t.view({2: torch.int16, 4: torch.int32, 8: torch.int64}[t.element_size()])
 
 
 def set_l2_fetch_granularity(nbytes: int) -> int:
@@ -190,9 +214,10 @@ class _OaBase:
         vb = 0 if value_dtype is None else _dtype_bytes(value_dtype)
         self.key_bytes, self.value_bytes = kb, vb
         self.empty_key, self.empty_value = empty_key, empty_value
-        d = OaDesc(kb, vb, bucket_size, probing, hash_kind, 0, _bits(empty_key, kb),
-                   _bits(empty_value, vb) if vb else 0,
-                   _bits(empty_key if erased_key is None else erased_key, kb))
+        fk, fv = _is_float(key_dtype), _is_float(value_dtype)
+        d = OaDesc(kb, vb, bucket_size, probing, hash_kind, KEY_FLOAT if fk else KEY_INTEGER, _bits(empty_key, kb, fk),
+                   _bits(empty_value, vb, fv) if vb else 0,
+                   _bits(empty_key if erased_key is None else erased_key, kb, fk))
         self._desc = d
         h = C.c_void_p()
         _call("b2co_oa_create", C.byref(d), C.c_uint64(capacity), _stream(stream), C.byref(h))
@@ -224,7 +249,8 @@ class _OaBase:
         return _device_bytes(self.Data(), self.Capacity() * self.slot_bytes())
 
     def SetErasedKey(self, erased_key, stream=None):
-        _call("b2co_oa_set_erased_key", self._h, C.c_uint64(_bits(erased_key, self.key_bytes)), _stream(stream))
+        _call("b2co_oa_set_erased_key", self._h,
+              C.c_uint64(_bits(erased_key, self.key_bytes, _is_float(self.key_dtype))), _stream(stream))
 
     def Clear(self, stream=None):
         _call("b2co_oa_clear", self._h, _stream(stream))
@@ -321,6 +347,10 @@ class _OaBase:
         flags = (FIND_SEGMENTED if segmented else 0) | (FIND_BULK if bulk else 0) | \
             (FIND_WARP_STAGED if warp_staged else 0) | (FIND_DEFERRED if deferred else 0)
         _call("b2co_oa_set_find_shape", self._h, C.c_uint32(lanes_per_key), C.c_uint32(keys_per_lane | flags))
+
+    def set_write_shape(self, lanes_per_key: int, keys_per_tile: int):
+        """Kernel shape of the insert family (b2co_oa_set_write_shape); (0, 0) = default."""
+        _call("b2co_oa_set_write_shape", self._h, C.c_uint32(lanes_per_key), C.c_uint32(keys_per_tile))
 
     @staticmethod
     def _n(t, n):

@@ -23,18 +23,20 @@ LIB = os.path.join(HERE, "lib", "libb2co.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
-         "-diag-suppress", "177", "-I", os.path.join(REPO, "include")]
+         "-diag-suppress", "177,128", "-I", os.path.join(REPO, "include")]
 
 
-def _deps_mtime() -> float:
-    files = (glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(REPO, "include", "*.h"))
+def _headers_mtime() -> float:
+    files = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+             + glob.glob(os.path.join(CSRC, "*.inc")) + glob.glob(os.path.join(REPO, "include", "*.h"))
              + glob.glob(os.path.join(REPO, "include", "b2co", "*")))
     return max(os.path.getmtime(f) for f in files)
 
 
 def _compile(src: str, force: bool, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime():
+    newest = max(_headers_mtime(), os.path.getmtime(src), os.path.getmtime(__file__))
+    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return obj
     cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
     if verbose:

@@ -23,6 +23,12 @@ struct WaitCtl {
 // Atomic compare-and-swap of a whole slot: 32-, 64- or 128-bit (the 128-bit form
 // needs sm_90+; it publishes key and payload together, so no reader ever sees a
 // key without its payload).
+// 2-byte slots (the narrow CAS of open_addressing_ref_impl.h:187-199) use the
+// native 16-bit compare-and-swap of sm_70+.
+__device__ __forceinline__ unsigned short cas_slot(unsigned short* p, unsigned short e, unsigned short d)
+{
+    return atomicCAS(p, e, d);
+}
 __device__ __forceinline__ uint32_t cas_slot(uint32_t* p, uint32_t e, uint32_t d) { return atomicCAS(p, e, d); }
 __device__ __forceinline__ unsigned long long cas_slot(unsigned long long* p, unsigned long long e,
                                                        unsigned long long d)
@@ -32,25 +38,45 @@ __device__ __forceinline__ unsigned long long cas_slot(unsigned long long* p, un
 __device__ __forceinline__ U128 cas_slot(U128* p, U128 e, U128 d) { return atomicCAS(p, e, d); }
 
 // Read-only (non-coherent) loads for kernels that never write the table, with
-// the 64-byte L2 prefetch-size hint: a bucket window is a random 80-byte read,
-// and larger fills only bring in neighbouring slots no query of this launch is
-// likely to touch.
+// an L2 prefetch-size hint (B2CO_RO_FILL bytes: 64 by default, 0 for none): a
+// bucket window is a random 80-byte read, and larger fills only bring in
+// neighbouring slots no query of this launch is likely to touch.
+#ifndef B2CO_RO_FILL
+#define B2CO_RO_FILL 64
+#endif
+#if B2CO_RO_FILL == 0
+#define B2CO_LD_RO "ld.global.nc"
+#elif B2CO_RO_FILL == 64
+#define B2CO_LD_RO "ld.global.nc.L2::64B"
+#elif B2CO_RO_FILL == 128
+#define B2CO_LD_RO "ld.global.nc.L2::128B"
+#elif B2CO_RO_FILL == 256
+#define B2CO_LD_RO "ld.global.nc.L2::256B"
+#else
+#error "B2CO_RO_FILL must be 0, 64, 128 or 256"
+#endif
+__device__ __forceinline__ unsigned short ld_ro(unsigned short const* p)
+{
+    unsigned short v;
+    asm(B2CO_LD_RO ".u16 %0, [%1];" : "=h"(v) : "l"(p));
+    return v;
+}
 __device__ __forceinline__ uint32_t ld_ro(uint32_t const* p)
 {
     uint32_t v;
-    asm("ld.global.nc.L2::64B.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    asm(B2CO_LD_RO ".u32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
 }
 __device__ __forceinline__ unsigned long long ld_ro(unsigned long long const* p)
 {
     unsigned long long v;
-    asm("ld.global.nc.L2::64B.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    asm(B2CO_LD_RO ".u64 %0, [%1];" : "=l"(v) : "l"(p));
     return v;
 }
 __device__ __forceinline__ U128 ld_ro(U128 const* p)
 {
     unsigned long long lo, hi;
-    asm("ld.global.nc.L2::64B.v2.u64 {%0, %1}, [%2];" : "=l"(lo), "=l"(hi) : "l"(p));
+    asm(B2CO_LD_RO ".v2.u64 {%0, %1}, [%2];" : "=l"(lo), "=l"(hi) : "l"(p));
     return U128{lo, hi};
 }
 // ---- bulk copies (TMA, untiled) and mbarriers --------------------------------
@@ -102,6 +128,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 
 // Coherent loads for kernels that race with writers to the same table.
+__device__ __forceinline__ unsigned short ld_rw(unsigned short const* p)
+{
+    return *reinterpret_cast<volatile unsigned short const*>(p);
+}
 __device__ __forceinline__ uint32_t ld_rw(uint32_t const* p) { return *reinterpret_cast<volatile uint32_t const*>(p); }
 __device__ __forceinline__ unsigned long long ld_rw(unsigned long long const* p)
 {

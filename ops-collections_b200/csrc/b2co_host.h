@@ -77,6 +77,15 @@ struct OaOps {
 };
 
 extern OaOps const kOpsSet4, kOpsSet8, kOpsMap44, kOpsMap48, kOpsMap84, kOpsMap88;
+// 2-byte-key layouts (integer and fp16 keys) and the floating-point-key layouts.
+extern OaOps const kOpsSet2, kOpsMap22, kOpsSet2F, kOpsMap22F, kOpsSet4F, kOpsMap44F, kOpsMap48F, kOpsSet8F,
+    kOpsMap84F, kOpsMap88F;
+
+// Launchers of a layout (nullptr for combinations without one).
+OaOps const* oa_ops_for(uint32_t key_bytes, uint32_t value_bytes, uint32_t key_kind);
+// Bytes of one slot: Pair<K,V> aligned to min(16, bitceil(sizeof K + sizeof V)),
+// the payload at the next offset aligned to its size (pair.inl:19-24), or a bare key.
+uint32_t oa_slot_bytes(uint32_t key_bytes, uint32_t value_bytes);
 
 struct GroupArgs;
 

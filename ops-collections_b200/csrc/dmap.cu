@@ -369,6 +369,8 @@ int b2co_dmap_create(b2co_oa_desc const* d, uint64_t initial_capacity, b2co_stre
     if (!d || !out) return fail(B2CO_EINVAL, "null descriptor or output");
     *out = nullptr;
     if (d->value_bytes == 0) return fail(B2CO_EINVAL, "DynamicMap needs a payload (value_bytes > 0)");
+    if (d->key_kind != B2CO_KEY_INTEGER || d->key_bytes < 4 || d->value_bytes < 4)
+        return fail(B2CO_EINVAL, "DynamicMap takes 4- or 8-byte integer keys and payloads");
     uint64_t kmask = d->key_bytes >= 8 ? ~0ull : ((1ull << (8 * d->key_bytes)) - 1);
     if ((d->empty_key_bits & kmask) == (d->erased_key_bits & kmask))
         return fail(B2CO_EINVAL, "DynamicMap: emptyKey and erasedKey must differ");

@@ -100,8 +100,9 @@ int b2co_oa_group_create(b2co_oa_desc const* d, uint64_t const* requested, uint3
     GroupOps const* gops = nullptr;
     OaOps const* ops = ops_for(d->key_bytes, d->value_bytes, &gops);
     if (!ops) return fail(B2CO_EINVAL, "unsupported key/value sizes");
-    if (d->probing > B2CO_PROBE_DOUBLE || d->hash > B2CO_HASH_XXH64 || d->reserved)
+    if (d->probing > B2CO_PROBE_DOUBLE || d->hash > B2CO_HASH_XXH64)
         return fail(B2CO_EINVAL, "bad descriptor");
+    if (d->key_kind != B2CO_KEY_INTEGER) return fail(B2CO_EINVAL, "table groups take integer keys");
     auto* g = new (std::nothrow) b2co_oa_group;
     if (!g) return fail(B2CO_ENOMEM, "host allocation failed");
     std::unique_ptr<b2co_oa_group, int (*)(b2co_oa_group*)> guard(g, b2co_oa_group_destroy);

@@ -11,15 +11,15 @@
 // Costs and rules that come with the fixed array:
 //  * every GPU that loads the library holds kNoAllocScratchBytes of device
 //    memory for the array until the process exits;
-//  * the first call on a device looks up the array's device address on that
-//    device (cudaGetSymbolAddress); make that first call before any stream
+//  * every call looks up the array's device address on the current device
+//    (cudaGetSymbolAddress, which allocates nothing), so an address cached
+//    across a device reset is never used; the first call on a device also
+//    loads the array there, so make that first call before any stream
 //    capture begins;
 //  * all calls share the one array and it keeps the last call's contents:
 //    calls that overlap on the GPU (other streams, other threads) race and
 //    must be serialized by the caller;
 //  * a batch whose scratch need exceeds the array is rejected with B2CO_ERANGE.
-#include <mutex>
-
 #include "b2co_host.h"
 
 int b2co_oa_iaf_first_wins_on(b2co_oa_table* t, void const* pairs, void* out_found, uint8_t* out_inserted, uint64_t n,
@@ -31,25 +31,17 @@ constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_mu;
-void* g_scratch_on_device[128] = {nullptr};
-
 size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up on
+// every call: a device reset reloads the module and may move the array.
 int scratch_address(void** out)
 {
-    int dev = 0;
-    B2CO_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 128) return b2co::fail(B2CO_EINVAL, "device ordinal out of range");
-    std::lock_guard<std::mutex> g(g_mu);
-    if (!g_scratch_on_device[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return b2co::cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
-        g_scratch_on_device[dev] = p;
-    }
-    *out = g_scratch_on_device[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return b2co::cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+    *out = p;
     return B2CO_OK;
 }
 

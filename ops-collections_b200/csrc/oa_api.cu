@@ -12,6 +12,42 @@
 
 using namespace b2co;
 
+namespace b2co {
+
+OaOps const* oa_ops_for(uint32_t kb, uint32_t vb, uint32_t kind)
+{
+    if (kind == B2CO_KEY_INTEGER) {
+        if (kb == 2 && vb == 0) return &kOpsSet2;
+        if (kb == 2 && vb == 2) return &kOpsMap22;
+        if (kb == 4 && vb == 0) return &kOpsSet4;
+        if (kb == 8 && vb == 0) return &kOpsSet8;
+        if (kb == 4 && vb == 4) return &kOpsMap44;
+        if (kb == 4 && vb == 8) return &kOpsMap48;
+        if (kb == 8 && vb == 4) return &kOpsMap84;
+        if (kb == 8 && vb == 8) return &kOpsMap88;
+    } else if (kind == B2CO_KEY_FLOAT) {
+        if (kb == 2 && vb == 0) return &kOpsSet2F;
+        if (kb == 2 && vb == 2) return &kOpsMap22F;
+        if (kb == 4 && vb == 0) return &kOpsSet4F;
+        if (kb == 4 && vb == 4) return &kOpsMap44F;
+        if (kb == 4 && vb == 8) return &kOpsMap48F;
+        if (kb == 8 && vb == 0) return &kOpsSet8F;
+        if (kb == 8 && vb == 4) return &kOpsMap84F;
+        if (kb == 8 && vb == 8) return &kOpsMap88F;
+    }
+    return nullptr;
+}
+
+uint32_t oa_slot_bytes(uint32_t kb, uint32_t vb)
+{
+    if (vb == 0) return kb;
+    uint32_t const sum = kb + vb, align = sum <= 4 ? 4 : (sum <= 8 ? 8 : 16);
+    uint32_t const end = (kb + vb - 1) / vb * vb + vb;
+    return (end + align - 1) / align * align;
+}
+
+}  // namespace b2co
+
 // Staging slots (and pipeline streams) of the host-buffer Find.
 constexpr int kHostSlots = 3;
 
@@ -40,22 +76,7 @@ namespace {
 
 uint64_t mask_bytes(uint64_t v, uint32_t n) { return n >= 8 ? v : (v & ((1ull << (8 * n)) - 1ull)); }
 
-OaOps const* ops_for(uint32_t kb, uint32_t vb)
-{
-    if (kb == 4 && vb == 0) return &kOpsSet4;
-    if (kb == 8 && vb == 0) return &kOpsSet8;
-    if (kb == 4 && vb == 4) return &kOpsMap44;
-    if (kb == 4 && vb == 8) return &kOpsMap48;
-    if (kb == 8 && vb == 4) return &kOpsMap84;
-    if (kb == 8 && vb == 8) return &kOpsMap88;
-    return nullptr;
-}
-
-uint32_t slot_bytes(uint32_t kb, uint32_t vb)
-{
-    if (vb == 0) return kb;
-    return (kb == 4 && vb == 4) ? 8 : 16;
-}
+uint32_t slot_bytes(uint32_t kb, uint32_t vb) { return oa_slot_bytes(kb, vb); }
 
 int check_table(b2co_oa_table const* t)
 {
@@ -82,7 +103,7 @@ void default_shape(b2co_oa_table* t)
         // queued and followed a pass at a time; four lanes per window (a 64-byte
         // row of 16-byte slots per load) with two windows in flight, or two
         // lanes and one window for 4-byte slots (measured best per layout)
-        bool const narrow = slot_bytes(t->desc.key_bytes, t->desc.value_bytes) == 4;
+        bool const narrow = slot_bytes(t->desc.key_bytes, t->desc.value_bytes) <= 4;
         t->find_lanes = narrow ? 2 : 4;
         t->find_items = (narrow ? 1 : 2) | kShapeDeferred;
     }
@@ -185,12 +206,18 @@ int b2co_oa_create_ex(b2co_oa_desc const* d, uint64_t requested, bool clear, b2c
 {
     if (!d || !out) return fail(B2CO_EINVAL, "null descriptor or output");
     *out = nullptr;
-    if (d->key_bytes != 4 && d->key_bytes != 8) return fail(B2CO_EINVAL, "key_bytes must be 4 or 8");
-    if (d->value_bytes != 0 && d->value_bytes != 4 && d->value_bytes != 8)
-        return fail(B2CO_EINVAL, "value_bytes must be 0, 4 or 8");
+    if (d->key_bytes != 2 && d->key_bytes != 4 && d->key_bytes != 8)
+        return fail(B2CO_EINVAL, "key_bytes must be 2, 4 or 8");
+    if (d->value_bytes != 0 && d->value_bytes != 2 && d->value_bytes != 4 && d->value_bytes != 8)
+        return fail(B2CO_EINVAL, "value_bytes must be 0, 2, 4 or 8");
     if (d->probing > B2CO_PROBE_DOUBLE) return fail(B2CO_EINVAL, "unknown probing scheme");
     if (d->hash > B2CO_HASH_XXH64) return fail(B2CO_EINVAL, "unknown hash");
-    if (d->reserved != 0) return fail(B2CO_EINVAL, "reserved descriptor field must be 0");
+    if (d->key_kind > B2CO_KEY_FLOAT) return fail(B2CO_EINVAL, "unknown key kind");
+    if (d->hash == B2CO_HASH_FMIX && d->key_bytes == 2)
+        return fail(B2CO_EINVAL, "the Fmix hashes take 4- or 8-byte keys (hash_functions/utils.h:42-66)");
+    if (!oa_ops_for(d->key_bytes, d->value_bytes, d->key_kind))
+        return fail(B2CO_EINVAL, "unsupported key/payload layout (2-byte payloads need 2-byte keys; 2-byte keys take "
+                                 "no payload or a 2-byte one)");
     uint64_t cap = 0;
     int st = b2co_oa_valid_capacity(requested, d->bucket_size, d->probing, &cap);
     if (st) return st;
@@ -203,7 +230,7 @@ int b2co_oa_create_ex(b2co_oa_desc const* d, uint64_t requested, bool clear, b2c
     t->desc.empty_key_bits = mask_bytes(d->empty_key_bits, d->key_bytes);
     t->desc.erased_key_bits = mask_bytes(d->erased_key_bits, d->key_bytes);
     t->desc.empty_value_bits = mask_bytes(d->empty_value_bits, d->value_bytes ? d->value_bytes : 8);
-    t->ops = ops_for(d->key_bytes, d->value_bytes);
+    t->ops = oa_ops_for(d->key_bytes, d->value_bytes, d->key_kind);
     t->capacity = cap;
     cudaGetDevice(&t->device);
     default_shape(t);
@@ -588,6 +615,20 @@ int b2co_oa_set_find_shape(b2co_oa_table* t, uint32_t lanes, uint32_t items)
     if (k != 1 && k != 2 && k != 4) return fail(B2CO_EINVAL, "keys per lane must be 1, 2 or 4");
     t->find_lanes = lanes;
     t->find_items = items;
+    return B2CO_OK;
+}
+
+int b2co_oa_set_write_shape(b2co_oa_table* t, uint32_t lanes, uint32_t keys_per_tile)
+{
+    if (int st = check_table(t)) return st;
+    if (lanes == 0 && keys_per_tile == 0) {
+        t->args.write_shape = 0;
+        return B2CO_OK;
+    }
+    if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) return fail(B2CO_EINVAL, "lanes must be 1, 2, 4 or 8");
+    if (keys_per_tile != 1 && keys_per_tile != 2 && keys_per_tile != 4)
+        return fail(B2CO_EINVAL, "keys per lane group must be 1, 2 or 4");
+    t->args.write_shape = (lanes << 8) | keys_per_tile;
     return B2CO_OK;
 }
 

@@ -5,6 +5,7 @@
 
 #include "b2co_host.h"
 #include "group_kernels.cuh"
+#include "oa_insert.cuh"
 #include "oa_kernels.cuh"
 
 namespace b2co {
@@ -12,6 +13,10 @@ namespace b2co {
 template <class S>
 struct OaImpl {
     static constexpr uint32_t kBlock = 256;
+    // The integer 4- and 8-byte layouts compile every lookup and write shape;
+    // 2-byte and floating-point-key layouts compile the default shapes only
+    // (another requested shape runs the default one).
+    static constexpr bool kAllShapes = !S::float_key && S::key_bytes >= 4;
 
     template <class F>
     static int with_b(uint32_t b, F&& f)
@@ -40,11 +45,43 @@ struct OaImpl {
         return check_launch("clear kernel");
     }
 
+    // Whether the insert family runs one key per lane (the scan of
+    // open_addressing_ref_impl.h:489-532 as written) instead of a tile per window.
+    static bool per_key_writes(OaArgs const& a, int B) { return B == 1 || (a.write_shape >> 8) == 1; }
+
+    // Cooperative-window write kernel (oa_insert.cuh) of the table's shape.
+    template <int B, int MODE>
+    static int launch_write(OaArgs const& a, void const* pairs, uint8_t const* stencil, uint32_t n, InsOut const& o,
+                            cudaStream_t s)
+    {
+        uint32_t lanes = a.write_shape >> 8, items = a.write_shape & 0xffu;
+        if (lanes == 0) lanes = 4, items = 2;
+        void (*k)(OaArgs, void const*, uint8_t const*, uint32_t, InsOut) = nullptr;
+        if constexpr (kAllShapes && B == 5) {  // other shapes: the common bucket size only (build time)
+            if (lanes == 2) k = items >= 2 ? k_insert_win<S, B, 2, 2, MODE> : k_insert_win<S, B, 2, 1, MODE>;
+            else if (lanes == 8) k = items >= 4 ? k_insert_win<S, B, 8, 4, MODE> : k_insert_win<S, B, 8, 2, MODE>;
+            else if (items == 1) k = k_insert_win<S, B, 4, 1, MODE>;
+            else if (items >= 4) k = k_insert_win<S, B, 4, 4, MODE>;
+        }
+        if (!k) lanes = 4, items = 2, k = k_insert_win<S, B, 4, 2, MODE>;
+        uint64_t const per_block = (kBlock / 32) * (32 / lanes) * items;
+        k<<<grid_for((void const*)k, kBlock, n, per_block), kBlock, 0, s>>>(a, pairs, stencil, n, o);
+        return check_launch("insert kernel");
+    }
+
     static int insert(OaArgs const& a, uint32_t b, void const* pairs, uint8_t const* stencil, uint32_t n,
                       bool assign, unsigned long long* counters, cudaStream_t s)
     {
         return with_b(b, [&](auto bc) {
             constexpr int B = decltype(bc)::value;
+            if constexpr (B > 1) {
+                if (!per_key_writes(a, B)) {
+                    InsOut o{};
+                    o.counters = counters;
+                    return assign ? launch_write<B, kInsAssign>(a, pairs, stencil, n, o, s)
+                                  : launch_write<B, kInsPlain>(a, pairs, stencil, n, o, s);
+                }
+            }
             auto k = assign ? k_insert<S, B, true> : k_insert<S, B, false>;
             k<<<grid_for((void const*)k, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, stencil, n, counters);
             return check_launch("insert kernel");
@@ -67,6 +104,14 @@ struct OaImpl {
     {
         return with_b(b, [&](auto bc) {
             constexpr int B = decltype(bc)::value;
+            if constexpr (B > 1) {
+                if (!per_key_writes(a, B)) {
+                    InsOut o{};
+                    o.found = found;
+                    o.inserted = inserted;
+                    return launch_write<B, kInsIafRace>(a, pairs, nullptr, n, o, s);
+                }
+            }
             auto k = k_iaf_race<S, B>;
             k<<<grid_for((void const*)k, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, found, inserted, n);
             return check_launch("insert_and_find kernel");
@@ -78,8 +123,21 @@ struct OaImpl {
     {
         return with_b(b, [&](auto bc) {
             constexpr int B = decltype(bc)::value;
-            auto k1 = k_iaf_place<S, B>;
-            k1<<<grid_for((void const*)k1, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, n, pos, newbits, owner);
+            bool placed = false;
+            if constexpr (B > 1) {
+                if (!per_key_writes(a, B)) {
+                    InsOut o{};
+                    o.pos = pos;
+                    o.newbits = newbits;
+                    o.owner = owner;
+                    if (int st = launch_write<B, kInsIafPlace>(a, pairs, nullptr, n, o, s)) return st;
+                    placed = true;
+                }
+            }
+            if (!placed) {
+                auto k1 = k_iaf_place<S, B>;
+                k1<<<grid_for((void const*)k1, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, n, pos, newbits, owner);
+            }
             auto k2 = k_iaf_min<S>;
             k2<<<grid_for((void const*)k2, kBlock, n, kBlock), kBlock, 0, s>>>(pos, newbits, owner, n);
             auto k3 = k_iaf_final<S>;
@@ -156,9 +214,48 @@ struct OaImpl {
         }
     }
 
+    // The default lookup shapes only (layouts without kAllShapes): per-warp
+    // staging with deferred continuations, 2 or 4 lanes per window, one or two
+    // windows in flight; the ballot tile (stencils, unaligned key streams) or
+    // one lane per key (bucket size 1) otherwise.
+    template <int B, bool C>
+    static int find_default(OaArgs const& a, uint32_t lanes, uint32_t items, void const* keys,
+                            uint8_t const* stencil, void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
+    {
+        bool const staged = !stencil && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 && n >= kWarpStageKeys &&
+                            B > 1 && lanes >= 2;
+        uint32_t const q = (items & ~(kShapeDeferred | kShapeWarpStaged | kShapeSegmented | kShapeBulk)) >= 2 ? 2 : 1;
+        if (staged) {
+            void (*k)(OaArgs, void const*, void*, uint32_t, WaitCtl) = nullptr;
+            if (lanes == 2) k = q == 2 ? k_find_wdefer<S, B, 2, 2, C> : k_find_wdefer<S, B, 2, 1, C>;
+            else k = q == 2 ? k_find_wdefer<S, B, 4, 2, C> : k_find_wdefer<S, B, 4, 1, C>;
+            uint64_t warps = (n + kWarpStageKeys - 1) / kWarpStageKeys;
+            k<<<grid_for((void const*)k, kBlock, warps ? warps : 1, kBlock / 32), kBlock, 0, s>>>(a, keys, out, n, wc);
+            return check_launch(C ? "contains kernel" : "find kernel");
+        }
+        void (*k)(OaArgs, void const*, uint8_t const*, void*, uint32_t) = nullptr;
+        uint64_t per_block = kBlock;
+        if (B == 1 || lanes <= 1) k = k_find_lane<S, B, 1, C>;
+        else if (lanes == 2) k = k_find_tile<S, B, 2, C>, per_block /= 2;
+        else k = k_find_tile<S, B, 4, C>, per_block /= 4;
+        k<<<grid_for((void const*)k, kBlock, n, per_block), kBlock, 0, s>>>(a, keys, stencil, out, n);
+        return check_launch(C ? "contains kernel" : "find kernel");
+    }
+
     template <int B, bool C>
     static int find_shape(OaArgs const& a, uint32_t lanes, uint32_t items, void const* keys, uint8_t const* stencil,
                           void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
+    {
+        if constexpr (!kAllShapes) {
+            return find_default<B, C>(a, lanes, items, keys, stencil, out, n, wc, s);
+        } else {
+            return find_any<B, C>(a, lanes, items, keys, stencil, out, n, wc, s);
+        }
+    }
+
+    template <int B, bool C>
+    static int find_any(OaArgs const& a, uint32_t lanes, uint32_t items, void const* keys, uint8_t const* stencil,
+                        void* out, uint32_t n, WaitCtl wc, cudaStream_t s)
     {
         bool const stageable = !stencil && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 && n >= kStageKeys && B > 1;
         // bulk-window path: 16-byte slots only
@@ -291,4 +388,11 @@ struct GroupImpl {
     namespace b2co {                                       \
     OaOps const NAME = OaImpl<SlotT<KB, VB>>::ops;         \
     GroupOps const GNAME = GroupImpl<SlotT<KB, VB>>::ops;  \
+    }
+
+// Layouts served by single tables only (no table-group kernels): 2-byte keys
+// and floating-point keys (FK = true).
+#define B2CO_DEFINE_OA_OPS_ONLY(NAME, KB, VB, FK)          \
+    namespace b2co {                                       \
+    OaOps const NAME = OaImpl<SlotT<KB, VB, FK>>::ops;     \
     }

@@ -35,10 +35,12 @@ struct OaArgs {
     uint64_t empty_key;
     uint64_t empty_value;
     uint64_t erased_key;
+    uint32_t write_shape;  // insert-family kernel shape: 0 = default, else (lanes << 8) | keys per tile
 };
 
 template <int N>
-using WordT = typename std::conditional<N == 8, unsigned long long, uint32_t>::type;
+using WordT = typename std::conditional<N == 8, unsigned long long,
+              typename std::conditional<N == 2, unsigned short, uint32_t>::type>::type;
 
 template <class S>
 struct Io {
@@ -94,18 +96,21 @@ __device__ __forceinline__ typename S::Raw insert_desired(typename S::Raw cur, u
 }
 
 // Payload store of an existing key (AssignPayload, open_addressing_ref_impl.h:208-220):
-// a whole-slot store for slots up to 8 bytes, the payload field otherwise.
+// a whole-slot store for slots up to 8 bytes, the payload field (at byte 8)
+// of a 16-byte slot otherwise.
 template <class S>
 __device__ __forceinline__ void assign_payload(typename S::Raw* slot, uint64_t k, uint64_t v)
 {
     if constexpr (S::is_set) {
         return;
-    } else if constexpr (S::bytes == 8) {
-        *reinterpret_cast<volatile unsigned long long*>(slot) = (unsigned long long)S::make(k, v);
+    } else if constexpr (S::bytes <= 8) {
+        *reinterpret_cast<volatile typename S::Raw*>(slot) = S::make(k, v);
     } else if constexpr (S::value_bytes == 8) {
         reinterpret_cast<volatile unsigned long long*>(slot)[1] = v;
-    } else {
+    } else if constexpr (S::value_bytes == 4) {
         reinterpret_cast<volatile uint32_t*>(slot)[2] = uint32_t(v);
+    } else {
+        reinterpret_cast<volatile unsigned short*>(slot)[4] = (unsigned short)v;
     }
 }
 
@@ -142,7 +147,7 @@ __device__ __forceinline__ int insert_one(OaArgs const& a, uint64_t key, uint64_
             Raw* sp = slots + idx + j;
             Raw cur = ld_rw(sp);
             uint64_t k = S::key(cur);
-            if (k == key) {
+            if (S::key_eq(k, key)) {
                 if constexpr (ASSIGN) assign_payload<S>(sp, key, val);
                 return kDuplicate;
             }
@@ -151,7 +156,7 @@ __device__ __forceinline__ int insert_one(OaArgs const& a, uint64_t key, uint64_
                 if (!insert_expected<S>(a, cur, expected)) continue;
                 Raw old = cas_slot(sp, expected, insert_desired<S>(cur, key, val));
                 if (raw_eq(old, expected)) return kSuccess;
-                if (S::key(old) == key) {
+                if (S::key_eq(S::key(old), key)) {
                     if constexpr (ASSIGN) assign_payload<S>(sp, key, val);
                     return kDuplicate;
                 }
@@ -215,7 +220,7 @@ __global__ void __launch_bounds__(256) k_assign_if(__grid_constant__ const OaArg
                 Raw* sp = slots + idx + j;
                 uint64_t k = S::key(ld_rw(sp));
                 if (k == a.empty_key) done = true;
-                else if (k == key) {
+                else if (S::key_eq(k, key)) {
                     assign_payload<S>(sp, key, S::value(p));
                     done = true;
                 }
@@ -255,7 +260,7 @@ __global__ void __launch_bounds__(256) k_iaf_race(__grid_constant__ const OaArgs
                     Raw* sp = slots + idx + j;
                     Raw cur = ld_rw(sp);
                     uint64_t k = S::key(cur);
-                    if (k == key) {
+                    if (S::key_eq(k, key)) {
                         found = S::value(settle<S>(a, sp, cur));
                         done = true;
                     } else if (k == a.empty_key) {
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(256) k_iaf_race(__grid_constant__ const OaArgs
                             found = S::is_set ? key : val;
                             inserted = 1;
                             done = true;
-                        } else if (S::key(old) == key) {
+                        } else if (S::key_eq(S::key(old), key)) {
                             found = S::value(old);
                             done = true;
                         }
@@ -316,7 +321,7 @@ __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArg
                     Raw* sp = slots + idx + j;
                     Raw cur = ld_rw(sp);
                     uint64_t k = S::key(cur);
-                    if (k == key) {
+                    if (S::key_eq(k, key)) {
                         where = idx + j;
                         done = true;
                     } else if (k == a.empty_key) {
@@ -328,7 +333,7 @@ __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArg
                             atomicOr(newbits + (where >> 5), 1u << (where & 31));
                             owner[where] = i;
                             done = true;
-                        } else if (S::key(old) == key) {
+                        } else if (S::key_eq(S::key(old), key)) {
                             where = idx + j;
                             done = true;
                         }
@@ -401,7 +406,7 @@ __device__ __forceinline__ bool scan_window(typename S::Raw const (&w)[B], uint6
 #pragma unroll
     for (int j = B - 1; j >= 0; --j) {
         uint64_t k = S::key(w[j]);
-        if (k == empty_key || k == key) {
+        if (k == empty_key || S::key_eq(k, key)) {
             stop = w[j];
             found = true;
         }
@@ -519,7 +524,7 @@ __global__ void __launch_bounds__(256) k_find_tile(__grid_constant__ const OaArg
                     w[t] = ld_ro(slots + idx + j);
                     k = S::key(w[t]);
                 }
-                bool is_hit = own && k == key && k != a.empty_key;
+                bool is_hit = own && S::key_eq(k, key) && k != a.empty_key;
                 bool is_stop = own && (k == a.empty_key || is_hit);
                 stop_bits |= ((__ballot_sync(0xffffffffu, is_stop) >> tile_shift) & TILE_MASK) << (t * G);
                 hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> tile_shift) & TILE_MASK) << (t * G);
@@ -582,7 +587,7 @@ __device__ __forceinline__ void tile_resolve(OaArgs const& a, typename S::Raw co
     for (int t = 0; t < ROUNDS; ++t) {
         bool const own = !skip && int(r) + t * G < B;
         uint64_t const k = own ? S::key(w[t]) : 0;
-        bool const is_stop = own && (k == a.empty_key || k == key);
+        bool const is_stop = own && (k == a.empty_key || S::key_eq(k, key));
         bool const is_hit = is_stop && k != a.empty_key;
         stop_bits |= ((__ballot_sync(0xffffffffu, is_stop) >> lane0) & MASK) << (t * G);
         hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> lane0) & MASK) << (t * G);
@@ -630,7 +635,7 @@ __device__ __forceinline__ void resolve_range(OaArgs const& a, typename S::Raw c
     for (int t = 0; t < ROUNDS; ++t) {
         bool const own = !skip && lo + int(r) + t * G < hi;
         uint64_t const k = own ? S::key(w[t]) : 0;
-        bool const is_stop = own && (k == a.empty_key || k == key);
+        bool const is_stop = own && (k == a.empty_key || S::key_eq(k, key));
         bool const is_hit = is_stop && k != a.empty_key;
         stop_bits |= ((__ballot_sync(0xffffffffu, is_stop) >> lane0) & MASK) << (t * G);
         hit_bits |= ((__ballot_sync(0xffffffffu, is_hit) >> lane0) & MASK) << (t * G);
@@ -989,7 +994,7 @@ __device__ __forceinline__ int tile_first_stop(typename S::Raw const (&w)[ROUNDS
     for (int t = ROUNDS - 1; t >= 0; --t) {
         if (!skip && int(r) + t * G < B) {
             uint64_t const k = S::key(w[t]);
-            if (k == empty_key || k == key) {
+            if (k == empty_key || S::key_eq(k, key)) {
                 own = int(r) + t * G;
                 mine = w[t];
             }
@@ -1001,8 +1006,13 @@ __device__ __forceinline__ int tile_first_stop(typename S::Raw const (&w)[ROUNDS
     return s;
 }
 
+// Resident blocks per SM the deferred lookup is compiled for (register cap).
+#ifndef B2CO_WDEFER_MINB
+#define B2CO_WDEFER_MINB(Q) ((Q) == 1 ? 4 : 3)
+#endif
+
 template <class S, int B, int G, int Q, bool CONTAINS>
-__global__ void __launch_bounds__(256, Q == 1 ? 4 : 3) k_find_wdefer(__grid_constant__ const OaArgs a, void const* keys, void* out,
+__global__ void __launch_bounds__(256, B2CO_WDEFER_MINB(Q)) k_find_wdefer(__grid_constant__ const OaArgs a, void const* keys, void* out,
                                                         uint32_t n, WaitCtl wc)
 {
     static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");
@@ -1283,7 +1293,7 @@ __global__ void __launch_bounds__(256) k_find_bulk(__grid_constant__ const OaArg
 #pragma unroll
                 for (int s = B - 1; s >= 0; --s) {
                     uint64_t k = S::key(w[s]);
-                    if (k == a.empty_key || k == key[j]) stop = s;
+                    if (k == a.empty_key || S::key_eq(k, key[j])) stop = s;
                 }
                 if (stop >= 0) {
                     hit = S::key(w[stop]) != a.empty_key;
@@ -1370,7 +1380,7 @@ __global__ void __launch_bounds__(256) k_erase(__grid_constant__ const OaArgs a,
                     if (tomb) done = true;
                     continue;
                 }
-                if (k == key) {
+                if (S::key_eq(k, key)) {
                     Raw desired;
                     if constexpr (S::bytes == 16) desired = insert_desired<S>(cur, target_key, a.empty_value);
                     else desired = S::make(target_key, a.empty_value);

@@ -184,6 +184,39 @@ int b2co_debug_set_wait(uint64_t limit_ns, int probe_timeout)
     return B2CO_OK;
 }
 
+// Host evaluation of the device-side key primitives (include/b2co/device.cuh).
+int b2co_probe_hash(uint32_t hash, uint32_t key_bytes, uint64_t key_bits, uint32_t seed, uint32_t* out)
+{
+    if (!out) return b2co::fail(B2CO_EINVAL, "output is null");
+    if (hash > B2CO_HASH_XXH64) return b2co::fail(B2CO_EINVAL, "unknown hash");
+    if (hash == B2CO_HASH_FMIX && key_bytes == 2) return b2co::fail(B2CO_EINVAL, "the Fmix hashes take 4 or 8 bytes");
+    switch (key_bytes) {
+        case 2: *out = b2co::probe_hash<2>(hash, key_bits & 0xffffu, seed); break;
+        case 4: *out = b2co::probe_hash<4>(hash, key_bits & 0xffffffffu, seed); break;
+        case 8: *out = b2co::probe_hash<8>(hash, key_bits, seed); break;
+        default: return b2co::fail(B2CO_EINVAL, "key_bytes must be 2, 4 or 8");
+    }
+    return B2CO_OK;
+}
+
+int b2co_key_equal(uint32_t key_kind, uint32_t key_bytes, uint64_t a_bits, uint64_t b_bits, int* equal)
+{
+    if (!equal) return b2co::fail(B2CO_EINVAL, "output is null");
+    if (key_kind > B2CO_KEY_FLOAT) return b2co::fail(B2CO_EINVAL, "unknown key kind");
+    uint64_t const m = key_bytes >= 8 ? ~0ull : ((1ull << (8 * key_bytes)) - 1ull);
+    a_bits &= m;
+    b_bits &= m;
+    bool r = false;
+    switch (key_bytes) {
+        case 2: r = key_kind ? b2co::key_equal<2, true>(a_bits, b_bits) : b2co::key_equal<2, false>(a_bits, b_bits); break;
+        case 4: r = key_kind ? b2co::key_equal<4, true>(a_bits, b_bits) : b2co::key_equal<4, false>(a_bits, b_bits); break;
+        case 8: r = key_kind ? b2co::key_equal<8, true>(a_bits, b_bits) : b2co::key_equal<8, false>(a_bits, b_bits); break;
+        default: return b2co::fail(B2CO_EINVAL, "key_bytes must be 2, 4 or 8");
+    }
+    *equal = r ? 1 : 0;
+    return B2CO_OK;
+}
+
 // MakeValidExtent (include/detail/extent/extent.inl:20-62).
 int b2co_oa_valid_capacity(uint64_t requested, uint32_t b, uint32_t probing, uint64_t* capacity)
 {

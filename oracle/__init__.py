@@ -64,6 +64,10 @@ def lib():
             "orc_find": (None, [vp, vp, vp, u64, vp, vp]),
             "orc_contains": (None, [vp, vp, vp, u64, vp, vp]),
             "orc_find_parallel": (None, [vp, vp, u64, vp, i32]),
+            "orc_contains_parallel": (None, [vp, vp, u64, vp, i32]),
+            "orc_key_equal": (i32, [i32, u32, u64, u64]),
+            "orc_pairs_match": (None, [vp, vp, vp, vp, vp, i32]),
+            "orc_group_check": (u64, [u64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32]),
             "orc_erase": (u64, [vp, vp, u64]),
             "orc_count": (u64, [vp, vp, u64]),
             "orc_bloom_add": (None, [vp, u64, vp, u32, u64, u64]),
@@ -91,9 +95,19 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+_UINT = {2: np.uint16, 4: np.uint32, 8: np.uint64}
+_FLOAT = {2: np.float16, 4: np.float32, 8: np.float64}
+
+
 def _bits(x, nbytes: int) -> int:
-    """Two's-complement bit pattern of an integer sentinel, as an unsigned value."""
+    """Bit pattern of a sentinel as an unsigned value: two's complement for
+    integers, the IEEE encoding of that width for floats."""
+    if isinstance(x, (float, np.floating)):
+        return int(np.array([x], dtype=_FLOAT[nbytes]).view(_UINT[nbytes])[0])
     return int(x) & ((1 << (8 * nbytes)) - 1)
+
+
+KEY_INT, KEY_FLOAT = 0, 1
 
 
 # ---- hashes ---------------------------------------------------------------
@@ -122,6 +136,11 @@ def probe_hash(kind: int, key_bits: int, key_bytes: int, seed: int) -> int:
     return lib().orc_probe_hash(kind, key_bits, key_bytes, seed)
 
 
+def key_equal(key_kind: int, key_bytes: int, a_bits: int, b_bits: int) -> bool:
+    """KeyEqual of a table of that key kind (KEY_INT bitwise, KEY_FLOAT IEEE ==) on bit patterns."""
+    return bool(lib().orc_key_equal(key_kind, key_bytes, a_bits, b_bits))
+
+
 def prime_table():
     n = lib().orc_prime_table_size()
     return np.array([lib().orc_prime_table_entry(i) for i in range(n)], dtype=np.uint64)
@@ -143,6 +162,7 @@ class _CTable(C.Structure):
         ("value_bytes", C.c_uint32), ("slot_bytes", C.c_uint32), ("value_offset", C.c_uint32),
         ("bucket_size", C.c_uint32), ("probing", C.c_int), ("hash_kind", C.c_int),
         ("empty_key", C.c_uint64), ("empty_value", C.c_uint64), ("erased_key", C.c_uint64),
+        ("key_kind", C.c_int),
     ]
 
 
@@ -155,8 +175,10 @@ def slot_layout(key_bytes: int, value_bytes: int):
 class Table:
     """A host open-addressing table with the reference's layout and semantics.
 
-    ``key_dtype``/``value_dtype`` are numpy integer dtypes; ``value_dtype`` None
-    makes a set.  ``capacity`` is the already-valid slot count (use
+    ``key_dtype``/``value_dtype`` are numpy integer or floating dtypes of 2, 4
+    or 8 bytes; ``value_dtype`` None makes a set.  Floating-point keys match
+    with IEEE ``==`` (so -0.0 finds +0.0 and NaN finds nothing); sentinels are
+    always compared bitwise.  ``capacity`` is the already-valid slot count (use
     :func:`valid_capacity` on a request first).
     """
 
@@ -169,11 +191,18 @@ class Table:
         vb = 0 if self.vdt is None else self.vdt.itemsize
         sb, vo = slot_layout(kb, vb)
         self.slots = np.zeros(capacity * sb, dtype=np.uint8)
+        fk = self.kdt.kind == "f"
+        if fk and not isinstance(empty_key, (float, np.floating)):
+            empty_key = float(empty_key)
+        if fk and erased_key is not None and not isinstance(erased_key, (float, np.floating)):
+            erased_key = float(erased_key)
+        if self.vdt is not None and self.vdt.kind == "f" and not isinstance(empty_value, (float, np.floating)):
+            empty_value = float(empty_value)
         ek = _bits(empty_key, kb)
         self.c = _CTable(
             _p(self.slots), capacity, kb, vb, sb, vo, bucket_size, probing, hash_kind,
             ek, _bits(empty_value, vb) if vb else 0,
-            ek if erased_key is None else _bits(erased_key, kb))
+            ek if erased_key is None else _bits(erased_key, kb), KEY_FLOAT if fk else KEY_INT)
         lib().orc_table_clear(C.byref(self.c))
 
     @property
@@ -231,6 +260,20 @@ class Table:
         lib().orc_find_parallel(C.byref(self.c), _p(k), len(k), _p(out), threads)
         return out
 
+    def contains_parallel(self, keys, threads: int = 0):
+        k = self._k(keys)
+        out = np.empty(len(k), dtype=np.uint8)
+        lib().orc_contains_parallel(C.byref(self.c), _p(k), len(k), _p(out), threads)
+        return out
+
+    def same_pairs(self, other: "Table", threads: int = 0):
+        """(equal, occupied_self, occupied_other, mismatches): whether ``other``
+        (e.g. a device table's dump) stores exactly this table's pair set.
+        ``self``'s keys must be distinct (true of any table built by the oracle)."""
+        oa, ob, mm = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        lib().orc_pairs_match(C.byref(self.c), C.byref(other.c), C.byref(oa), C.byref(ob), C.byref(mm), threads)
+        return mm.value == 0 and oa.value == ob.value, oa.value, ob.value, mm.value
+
     def contains(self, keys, stencil=None):
         k, s = self._k(keys), self._s(stencil)
         out = np.empty(len(k), dtype=np.uint8)
@@ -263,19 +306,42 @@ class Table:
         return keys, vals
 
     def pairs(self):
-        """The stored pair set: sorted (key, value) rows of occupied slots."""
+        """The stored pair set: sorted (key bits, value bits) rows of occupied
+        slots (unsigned bit patterns, so floating-point keys sort and compare
+        exactly)."""
         keys, vals = self.slot_keys_values()
-        ek = np.array(self.c.empty_key, dtype=np.uint64).astype(self.kdt.str.replace("i", "u"))
-        kb = keys.view(self.kdt.str.replace("i", "u"))
-        occ = kb != ek
+        ut = _UINT[self.kdt.itemsize]
+        kb = keys.view(ut)
+        occ = kb != ut(self.c.empty_key)
         if self.c.erased_key != self.c.empty_key:
-            er = np.array(self.c.erased_key, dtype=np.uint64).astype(self.kdt.str.replace("i", "u"))
-            occ &= kb != er
+            occ &= kb != ut(self.c.erased_key)
         if vals is None:
-            return np.sort(keys[occ])
-        k, v = keys[occ], vals[occ]
+            return np.sort(kb[occ]).astype(np.uint64)
+        k, v = kb[occ].astype(np.uint64), vals[occ].view(_UINT[self.vdt.itemsize]).astype(np.uint64)
         order = np.lexsort((v, k))
-        return np.stack([k[order].astype(np.int64), v[order].astype(np.int64)], axis=1)
+        return np.stack([k[order], v[order]], axis=1)
+
+
+def group_check(caps, shape: Table, slab: np.ndarray, keys, values, ins_off, queries, q_off, threads: int = 0):
+    """The batched pattern checked table by table: every table is rebuilt by
+    the oracle from its own inserts (tables in parallel), its stored set is
+    compared with its segment of ``slab`` (the device group's slot dump, tables
+    back to back), and its queries are answered.  Returns (bad_tables,
+    first_bad_table_or_None, expected_find_outputs)."""
+    caps = np.ascontiguousarray(caps, dtype=np.uint64)
+    slot_off = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.uint64)
+    k = np.ascontiguousarray(keys, dtype=shape.kdt)
+    v = None if shape.vdt is None else np.ascontiguousarray(values, dtype=shape.vdt)
+    q = np.ascontiguousarray(queries, dtype=shape.kdt)
+    io = np.ascontiguousarray(ins_off, dtype=np.uint64)
+    qo = np.ascontiguousarray(q_off, dtype=np.uint64)
+    raw = np.ascontiguousarray(slab).view(np.uint8).reshape(-1)
+    assert raw.size == int(caps.sum()) * shape.c.slot_bytes
+    out = np.empty(len(q), dtype=shape._out_dtype())
+    first = C.c_uint64()
+    bad = lib().orc_group_check(len(caps), _p(caps), _p(slot_off), _p(raw), C.byref(shape.c), _p(k), _p(v), _p(io),
+                                _p(q), _p(qo), _p(out), C.byref(first), threads)
+    return int(bad), (None if bad == 0 else int(first.value)), out
 
 
 # ---- Bloom filter -----------------------------------------------------------

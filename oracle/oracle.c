@@ -130,7 +130,7 @@ uint32_t orc_probe_hash(int kind, uint64_t key_bits, uint32_t key_bytes, uint32_
     switch (kind) {
         case ORC_HASH_XXH32: return orc_xxh32(kb, key_bytes, seed);
         case ORC_HASH_MURMUR3_32: return orc_murmur3_32(kb, key_bytes, seed);
-        case ORC_HASH_FMIX:
+        case ORC_HASH_FMIX:  /* Fmix32/Fmix64 take 4- or 8-byte keys only (utils.h:42-66) */
             return key_bytes == 4 ? orc_fmix32((uint32_t)key_bits, seed) : (uint32_t)orc_fmix64(key_bits, seed);
         case ORC_HASH_XXH64: return (uint32_t)orc_xxh64(kb, key_bytes, seed);
     }
@@ -313,6 +313,37 @@ static inline void write_slot(orc_table* t, uint32_t i, uint64_t k, uint64_t v)
 }
 static inline uint64_t empty_payload(const orc_table* t) { return t->value_bytes ? t->empty_value : t->empty_key; }
 
+/* IEEE 754 binary16 -> binary32, exact (every half is a float). */
+static float half_to_float(uint16_t h)
+{
+    uint32_t e = (h >> 10) & 31u, m = h & 1023u;
+    float v;
+    if (e == 0) v = ldexpf((float)m, -24);
+    else if (e == 31) v = m ? NAN : INFINITY;
+    else v = ldexpf((float)(m | 1024u), (int)e - 25);
+    return (h >> 15) ? -v : v;
+}
+
+/* KeyEqual (EqualTo, utility/math_utils.h:66-70 via equal_wrapper.h:30-33):
+ * integer keys compare bitwise; floating-point keys with ==, so -0 matches +0
+ * and NaN matches nothing.  Sentinel tests stay bitwise everywhere. */
+static inline int key_eq(const orc_table* t, uint64_t a, uint64_t b)
+{
+    if (t->key_kind != ORC_KEY_FLOAT) return a == b;
+    if (t->key_bytes == 2) return half_to_float((uint16_t)a) == half_to_float((uint16_t)b);
+    if (t->key_bytes == 4) {
+        uint32_t ua = (uint32_t)a, ub = (uint32_t)b;
+        float x, y;
+        memcpy(&x, &ua, 4);
+        memcpy(&y, &ub, 4);
+        return x == y;
+    }
+    double x, y;
+    memcpy(&x, &a, 8);
+    memcpy(&y, &b, 8);
+    return x == y;
+}
+
 /* Storage initialisation: every slot holds Pair{emptyKey, emptyValue}
  * (open_addressing_impl.h:84-93, bucket_storage.inl:52-64). */
 void orc_table_clear(orc_table* t)
@@ -343,7 +374,7 @@ static int insert_verdict(orc_table* t, uint64_t key, uint64_t val, int assign, 
                 if (where) *where = s;
                 return ORC_SUCCESS;
             }
-            if (sk == key) {
+            if (key_eq(t, sk, key)) {
                 if (assign && t->value_bytes) st_bits(slot_ptr(t, s) + t->value_offset, val, t->value_bytes);
                 if (where) *where = s;
                 return ORC_DUPLICATE;
@@ -363,11 +394,34 @@ static inline uint64_t in_val(const orc_table* t, const void* vals, uint64_t i)
     return ld_bits((const uint8_t*)vals + i * t->value_bytes, t->value_bytes);
 }
 
+/* The sequential bulk forms touch the first bucket window of input i + kAhead
+ * early (a cache prefetch, no state change), so a large table is not walked at
+ * one DRAM latency per key; results are those of the plain in-order loop. */
+enum { kAhead = 16 };
+static inline void touch_first_window(const orc_table* t, const void* keys, uint64_t i, uint64_t n)
+{
+    if (i >= n) return;
+    orc_probe_iter it = iter_for(t, in_key(t, keys, i));
+    const uint8_t* p = slot_ptr(t, it.idx);
+    __builtin_prefetch(p, 1, 0);
+    __builtin_prefetch(p + (size_t)t->bucket_size * t->slot_bytes - 1, 1, 0);
+}
+
+int orc_key_equal(int key_kind, uint32_t key_bytes, uint64_t a, uint64_t b)
+{
+    orc_table t;
+    memset(&t, 0, sizeof t);
+    t.key_kind = key_kind;
+    t.key_bytes = key_bytes;
+    return key_eq(&t, a, b);
+}
+
 /* Insert / InsertIf: kernels.h:46-83; returns the failed count (pred-true items only). */
 uint64_t orc_insert(orc_table* t, const void* keys, const void* vals, const uint8_t* stencil, uint64_t n)
 {
     uint64_t failed = 0;
     for (uint64_t i = 0; i < n; ++i) {
+        touch_first_window(t, keys, i + kAhead, n);
         if (stencil && !stencil[i]) continue;
         if (insert_verdict(t, in_key(t, keys, i), in_val(t, vals, i), 0, NULL) != ORC_SUCCESS) ++failed;
     }
@@ -380,6 +434,7 @@ uint64_t orc_insert_or_assign(orc_table* t, const void* keys, const void* vals, 
 {
     uint64_t failed = 0, asg = 0;
     for (uint64_t i = 0; i < n; ++i) {
+        touch_first_window(t, keys, i + kAhead, n);
         int r = insert_verdict(t, in_key(t, keys, i), in_val(t, vals, i), 1, NULL);
         if (r == ORC_FAILED) ++failed;
         else if (r == ORC_DUPLICATE) ++asg;
@@ -402,7 +457,7 @@ void orc_assign_if(orc_table* t, const void* keys, const void* vals, const uint8
                 uint32_t s = it.idx + j;
                 uint64_t sk = slot_key(t, s);
                 if (sk == t->empty_key) { done = 1; break; }
-                if (sk == key) {
+                if (key_eq(t, sk, key)) {
                     st_bits(slot_ptr(t, s) + t->value_offset, in_val(t, vals, i), t->value_bytes);
                     done = 1;
                 }
@@ -420,6 +475,7 @@ void orc_insert_and_find(orc_table* t, const void* keys, const void* vals, uint6
 {
     uint32_t ob = t->value_bytes ? t->value_bytes : t->key_bytes;
     for (uint64_t i = 0; i < n; ++i) {
+        touch_first_window(t, keys, i + kAhead, n);
         uint64_t key = in_key(t, keys, i);
         uint32_t where = 0;
         int r = insert_verdict(t, key, in_val(t, vals, i), 0, &where);
@@ -441,7 +497,7 @@ static int find_one(const orc_table* t, uint64_t key, uint64_t* val, uint32_t* w
             uint32_t s = it.idx + i;
             uint64_t sk = slot_key(t, s);
             if (sk == t->empty_key) { *val = empty_payload(t); *windows = w; return 0; }
-            if (sk == key) { *val = slot_val(t, s); *windows = w; return 1; }
+            if (key_eq(t, sk, key)) { *val = slot_val(t, s); *windows = w; return 1; }
         }
         if (orc_iter_next(&it) == init) { *val = empty_payload(t); *windows = w; return 0; }
     }
@@ -474,6 +530,118 @@ void orc_find_parallel(const orc_table* t, const void* keys, uint64_t n, void* o
         st_bits((uint8_t*)out + (uint64_t)i * ob, v, ob);
     }
     (void)threads;
+}
+
+void orc_contains_parallel(const orc_table* t, const void* keys, uint64_t n, uint8_t* out, int threads)
+{
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(static, 65536)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        uint64_t v;
+        uint32_t w;
+        out[i] = (uint8_t)find_one(t, in_key(t, keys, (uint64_t)i), &v, &w);
+    }
+    (void)threads;
+}
+
+static inline int slot_occupied(const orc_table* t, uint32_t s)
+{
+    uint64_t k = slot_key(t, s);
+    return k != t->empty_key && (t->erased_key == t->empty_key || k != t->erased_key);
+}
+
+/* Slots [lo, hi) of a: occupied count, and keys b misses or holds with another payload. */
+static void pairs_match_range(const orc_table* a, const orc_table* b, uint32_t lo, uint32_t hi, uint64_t* occ,
+                              uint64_t* bad)
+{
+    for (uint32_t s = lo; s < hi; ++s) {
+        if (!slot_occupied(a, s)) continue;
+        ++*occ;
+        uint64_t v;
+        uint32_t w;
+        if (!find_one(b, slot_key(a, s), &v, &w) || v != slot_val(a, s)) ++*bad;
+    }
+}
+
+static uint64_t count_occupied(const orc_table* t)
+{
+    uint64_t c = 0;
+    for (uint32_t s = 0; s < t->capacity; ++s) c += (uint64_t)slot_occupied(t, s);
+    return c;
+}
+
+void orc_pairs_match(const orc_table* a, const orc_table* b, uint64_t* occupied_a, uint64_t* occupied_b,
+                     uint64_t* mismatches, int threads)
+{
+    uint64_t occ_a = 0, occ_b = 0, bad = 0;
+    int64_t const chunk = 1 << 20, nchunks = ((int64_t)a->capacity + chunk - 1) / chunk;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : occ_a, bad)
+#endif
+    for (int64_t c = 0; c < nchunks; ++c) {
+        uint64_t hi = (uint64_t)(c + 1) * chunk;
+        pairs_match_range(a, b, (uint32_t)(c * chunk), (uint32_t)(hi < a->capacity ? hi : a->capacity), &occ_a,
+                          &bad);
+    }
+    int64_t const nb = ((int64_t)b->capacity + chunk - 1) / chunk;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : occ_b)
+#endif
+    for (int64_t c = 0; c < nb; ++c) {
+        uint64_t hi = (uint64_t)(c + 1) * chunk;
+        for (uint32_t s = (uint32_t)(c * chunk); s < (uint32_t)(hi < b->capacity ? hi : b->capacity); ++s)
+            occ_b += (uint64_t)slot_occupied(b, s);
+    }
+    *occupied_a = occ_a;
+    *occupied_b = occ_b;
+    *mismatches = bad;
+    (void)threads;
+}
+
+uint64_t orc_group_check(uint64_t count, const uint64_t* caps, const uint64_t* slot_off, const uint8_t* slab,
+                         const orc_table* shape, const void* keys, const void* values, const uint64_t* ins_off,
+                         const void* queries, const uint64_t* q_off, void* out_expected, uint64_t* first_bad,
+                         int threads)
+{
+    uint64_t bad = 0, first = UINT64_MAX;
+    uint32_t const ob = shape->value_bytes ? shape->value_bytes : shape->key_bytes;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : bad)
+#endif
+    for (int64_t i = 0; i < (int64_t)count; ++i) {
+        orc_table o = *shape, d = *shape;
+        o.capacity = d.capacity = (uint32_t)caps[i];
+        o.slots = (uint8_t*)malloc((size_t)caps[i] * shape->slot_bytes);
+        d.slots = (uint8_t*)slab + slot_off[i] * shape->slot_bytes;
+        orc_table_clear(&o);
+        uint64_t const k0 = ins_off[i], nk = ins_off[i + 1] - k0;
+        orc_insert(&o, (const uint8_t*)keys + k0 * shape->key_bytes,
+                   values ? (const uint8_t*)values + k0 * shape->value_bytes : NULL, NULL, nk);
+        uint64_t occ = 0, mism = 0;
+        pairs_match_range(&o, &d, 0, o.capacity, &occ, &mism);
+        if (mism || count_occupied(&d) != occ) {
+            ++bad;
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+            if ((uint64_t)i < first) first = (uint64_t)i;
+        }
+        uint64_t const q0 = q_off[i];
+        for (uint64_t j = q0; j < q_off[i + 1]; ++j) {
+            uint64_t v;
+            uint32_t w;
+            find_one(&o, in_key(&o, queries, j), &v, &w);
+            st_bits((uint8_t*)out_expected + j * ob, v, ob);
+        }
+        free(o.slots);
+    }
+    if (first_bad) *first_bad = first;
+    (void)threads;
+    return bad;
 }
 
 /* ContainsIf (kernels.h:349-377). */
@@ -509,7 +677,7 @@ uint64_t orc_erase(orc_table* t, const void* keys, uint64_t n)
                     if (tomb) done = 1;
                     continue;
                 }
-                if (sk == key) {
+                if (key_eq(t, sk, key)) {
                     write_slot(t, s, tomb ? t->erased_key : t->empty_key, t->empty_value);
                     ok = 1;
                     done = 1;

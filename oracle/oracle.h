@@ -32,7 +32,8 @@ uint64_t orc_fmix64(uint64_t key, uint64_t seed);
 enum { ORC_HASH_XXH32 = 0, ORC_HASH_MURMUR3_32 = 1, ORC_HASH_FMIX = 2, ORC_HASH_XXH64 = 3 };
 enum { ORC_PROBE_LINEAR = 0, ORC_PROBE_DOUBLE = 1 };
 
-/* 32-bit probe hash of a key's object representation (key_bytes 4 or 8). */
+/* 32-bit probe hash of a key's object representation (key_bytes 2, 4 or 8;
+ * the Fmix family needs 4 or 8). */
 uint32_t orc_probe_hash(int hash_kind, uint64_t key_bits, uint32_t key_bytes, uint32_t seed);
 
 /* ---- capacity (include/detail/extent/extent.inl:20-62, utility/prime.h) */
@@ -56,9 +57,9 @@ uint32_t orc_iter_next(orc_probe_iter* it);
 typedef struct {
     uint8_t* slots;          /* capacity * slot_bytes bytes, owned by the caller */
     uint32_t capacity;
-    uint32_t key_bytes;      /* 4 or 8 */
-    uint32_t value_bytes;    /* 0 (set), 4 or 8 */
-    uint32_t slot_bytes;     /* 4, 8 or 16 */
+    uint32_t key_bytes;      /* 2, 4 or 8 */
+    uint32_t value_bytes;    /* 0 (set), 2, 4 or 8 */
+    uint32_t slot_bytes;     /* 2, 4, 8 or 16 */
     uint32_t value_offset;
     uint32_t bucket_size;
     int probing;
@@ -66,7 +67,15 @@ typedef struct {
     uint64_t empty_key;
     uint64_t empty_value;
     uint64_t erased_key;     /* == empty_key when no tombstone is configured */
+    int key_kind;            /* ORC_KEY_INT: bitwise key match; ORC_KEY_FLOAT: IEEE == (fp16/fp32/fp64) */
 } orc_table;
+
+/* Key kinds: the reference matches keys with KeyEqual (==, utility/equal_wrapper.h:30-33)
+ * and tests sentinels bitwise (:35-42; utility/traits.h:27-28). */
+enum { ORC_KEY_INT = 0, ORC_KEY_FLOAT = 1 };
+
+/* KeyEqual of a table of this key kind on two key bit patterns. */
+int orc_key_equal(int key_kind, uint32_t key_bytes, uint64_t a, uint64_t b);
 
 /* Slot layout of Pair<K,V> (pair.inl:19-24) or of a bare key. */
 void orc_slot_layout(uint32_t key_bytes, uint32_t value_bytes, uint32_t* slot_bytes, uint32_t* value_offset);
@@ -86,8 +95,28 @@ void orc_find(const orc_table* t, const void* keys, const uint8_t* stencil, uint
               uint32_t* out_windows);
 void orc_contains(const orc_table* t, const void* keys, const uint8_t* stencil, uint64_t n, uint8_t* out,
                   uint32_t* out_windows);
-/* Multi-threaded (OpenMP) read-only Find, used only as the timed CPU baseline. */
+/* Multi-threaded (OpenMP) read-only Find and Contains: the timed CPU baseline
+ * and the checker of full-size query streams. */
 void orc_find_parallel(const orc_table* t, const void* keys, uint64_t n, void* out_values, int threads);
+void orc_contains_parallel(const orc_table* t, const void* keys, uint64_t n, uint8_t* out, int threads);
+/* Stored-set comparison: every occupied slot of `a` (whose keys are distinct,
+ * e.g. the oracle's own table) is looked up in `b`; *mismatches counts keys
+ * that `b` misses or holds with another payload, *occupied_a / *occupied_b
+ * count the occupied (non-empty, non-tombstone) slots.  The two stored pair
+ * sets are equal exactly when mismatches == 0 and the counts agree. */
+void orc_pairs_match(const orc_table* a, const orc_table* b, uint64_t* occupied_a, uint64_t* occupied_b,
+                     uint64_t* mismatches, int threads);
+/* Many independent tables (the batched pattern): table i has capacity caps[i]
+ * (valid, slots in `slab` from slot offset slot_off[i]), inserts pairs
+ * [ins_off[i], ins_off[i+1]) of keys/values in order, then answers queries
+ * [q_off[i], q_off[i+1]).  Each table is rebuilt sequentially by the oracle
+ * (tables in parallel), its stored set compared with the slab's segment (the
+ * device's tables), and its Find results written to out_expected.  Returns the
+ * number of tables whose stored set differs; the first one goes to *first_bad. */
+uint64_t orc_group_check(uint64_t count, const uint64_t* caps, const uint64_t* slot_off, const uint8_t* slab,
+                         const orc_table* shape, const void* keys, const void* values, const uint64_t* ins_off,
+                         const void* queries, const uint64_t* q_off, void* out_expected, uint64_t* first_bad,
+                         int threads);
 uint64_t orc_erase(orc_table* t, const void* keys, uint64_t n);
 uint64_t orc_count(const orc_table* t, const void* keys, uint64_t n);
 

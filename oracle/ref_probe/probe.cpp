@@ -13,6 +13,8 @@
 #include "bloom_filter_policy.h"
 #include "detail/hyperloglog/finalizer.h"
 #include "roaring_bitmap_ref.h"
+#include "utility/equal_wrapper.h"
+#include "utility/math_utils.h"
 
 namespace {
 template <int B>
@@ -43,7 +45,9 @@ static void walk(int dh, int hash, Key key, uint32_t cap, uint32_t count, uint32
     } else if (hash == 1) {
         if (dh) run(aclco::DoubleHashing<aclco::murmurhash3_32<Key>>{}); else run(aclco::LinearProbing<aclco::murmurhash3_32<Key>>{});
     } else if (hash == 2) {
-        if constexpr (sizeof(Key) == 4) {
+        if constexpr (sizeof(Key) == 2) {
+            // the Fmix hashes static_assert 4- or 8-byte keys (utils.h:42-66): no walk
+        } else if constexpr (sizeof(Key) == 4) {
             if (dh) run(aclco::DoubleHashing<aclco::murmurhash3_fmix32<Key>>{}); else run(aclco::LinearProbing<aclco::murmurhash3_fmix32<Key>>{});
         } else {
             if (dh) run(aclco::DoubleHashing<aclco::murmurhash3_fmix64<Key>>{}); else run(aclco::LinearProbing<aclco::murmurhash3_fmix64<Key>>{});
@@ -51,6 +55,19 @@ static void walk(int dh, int hash, Key key, uint32_t cap, uint32_t count, uint32
     } else {
         if (dh) run(aclco::DoubleHashing<aclco::xxhash_64<Key>>{}); else run(aclco::LinearProbing<aclco::xxhash_64<Key>>{});
     }
+}
+// The reference's key comparison for floating-point keys, on bit patterns:
+// EqualWrapper<T, EqualTo<T>> (utility/equal_wrapper.h) returns 1 for EQUAL
+// from EqualTo and, from IsSentinelValue, whether the value is the sentinel.
+template <typename T, typename Bits>
+static int eq_of(Bits a, Bits b, int sentinel)
+{
+    T x, y;
+    std::memcpy(&x, &a, sizeof(T));
+    std::memcpy(&y, &b, sizeof(T));
+    aclco::EqualWrapper<T, aclco::EqualTo<T>> w{aclco::EqualTo<T>{}};
+    if (sentinel) return w.IsSentinelValue(x, y) ? 1 : 0;
+    return w.EqualTo(x, y) == aclco::EqualResult::EQUAL ? 1 : 0;
 }
 }  // namespace
 
@@ -64,6 +81,13 @@ uint64_t ref_xxh64_f32(float k, uint64_t seed) { return aclco::xxhash_64<float>{
 uint32_t ref_murmur3_u32(uint32_t k, uint32_t seed) { return aclco::murmurhash3_32<uint32_t>{seed}(k); }
 uint32_t ref_murmur3_u64(uint64_t k, uint32_t seed) { return aclco::murmurhash3_32<uint64_t>{seed}(k); }
 uint32_t ref_fmix32(uint32_t k, uint32_t seed) { return aclco::murmurhash3_fmix32<uint32_t>{seed}(k); }
+uint32_t ref_xxh32_u16(uint16_t k, uint32_t seed) { return aclco::xxhash_32<uint16_t>{seed}(k); }
+uint32_t ref_murmur3_u16(uint16_t k, uint32_t seed) { return aclco::murmurhash3_32<uint16_t>{seed}(k); }
+uint64_t ref_xxh64_u16(uint16_t k, uint64_t seed) { return aclco::xxhash_64<uint16_t>{seed}(k); }
+
+int ref_equal_f16(uint16_t a, uint16_t b, int sentinel) { return eq_of<_Float16>(a, b, sentinel); }
+int ref_equal_f32(uint32_t a, uint32_t b, int sentinel) { return eq_of<float>(a, b, sentinel); }
+int ref_equal_f64(uint64_t a, uint64_t b, int sentinel) { return eq_of<double>(a, b, sentinel); }
 uint64_t ref_fmix64(uint64_t k, uint64_t seed) { return aclco::murmurhash3_fmix64<uint64_t>{seed}(k); }
 
 uint64_t ref_prime_count() { return aclco::primes.size(); }
@@ -87,7 +111,14 @@ uint64_t ref_valid_capacity(uint64_t req, int b, int dh)
 
 void ref_probe_walk(int key_bytes, int b, int dh, int hash, uint64_t key, uint32_t cap, uint32_t count, uint32_t* out)
 {
-    if (key_bytes == 4) {
+    if (key_bytes == 2) {
+        uint16_t k = static_cast<uint16_t>(key);
+        switch (b) {
+            case 1: walk<uint16_t, 1>(dh, hash, k, cap, count, out); break;
+            case 5: walk<uint16_t, 5>(dh, hash, k, cap, count, out); break;
+            case 8: walk<uint16_t, 8>(dh, hash, k, cap, count, out); break;
+        }
+    } else if (key_bytes == 4) {
         uint32_t k = static_cast<uint32_t>(key);
         switch (b) {
             case 1: walk<uint32_t, 1>(dh, hash, k, cap, count, out); break;

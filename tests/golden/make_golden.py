@@ -6,7 +6,10 @@ in place, outputs into oracle/_ref/) and records their outputs as plain
 numbers.  The fixtures pin the oracle and the product; nothing here runs on
 the GPU box.
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <checkout of the reference project>
+
+(--ref defaults to the B2CO_REFERENCE environment variable, else to a
+`reference` directory beside this repository.)
 """
 from __future__ import annotations
 
@@ -32,6 +35,10 @@ def load_probe(ref: str):
         "ref_xxh64_u32": (u64, [u32, u64]), "ref_xxh64_u64": (u64, [u64, u64]),
         "ref_xxh64_i64": (u64, [i64, u64]), "ref_xxh64_f32": (u64, [C.c_float, u64]),
         "ref_murmur3_u32": (u32, [u32, u32]), "ref_murmur3_u64": (u32, [u64, u32]),
+        "ref_xxh32_u16": (u32, [C.c_uint16, u32]), "ref_murmur3_u16": (u32, [C.c_uint16, u32]),
+        "ref_xxh64_u16": (u64, [C.c_uint16, u64]),
+        "ref_equal_f16": (i32, [C.c_uint16, C.c_uint16, i32]), "ref_equal_f32": (i32, [u32, u32, i32]),
+        "ref_equal_f64": (i32, [u64, u64, i32]),
         "ref_fmix32": (u32, [u32, u32]), "ref_fmix64": (u64, [u64, u64]),
         "ref_prime_count": (u64, []), "ref_prime_at": (i64, [u64]),
         "ref_valid_capacity": (u64, [u64, i32, i32]),
@@ -88,7 +95,33 @@ def hashes(L, rng):
     out["xxh64_f32"] = [{"bits": b, "seed": 0,
                          "h": L.ref_xxh64_f32(np.array([b], np.uint32).view(np.float32)[0].item(), 0)}
                         for b in [0x00000000, 0x80000000, 0x3f800000, 0x7fc00000, 0xff800000]]
+    # 2-byte keys (int16/uint16/fp16 hash their two bytes): a fixed sample of the key space
+    r16 = np.random.default_rng(16)
+    keys16 = sorted(set([0, 1, 2, 0x7fff, 0x8000, 0xffff, 0x3c00, 0xbc00, 0x7c00, 0x7e00]
+                        + [int(x) for x in r16.integers(0, 1 << 16, size=200)]))
+    out["vectors16"] = [{"key": k, "seed": sd, "xxh32": L.ref_xxh32_u16(k, sd), "murmur3_32": L.ref_murmur3_u16(k, sd),
+                         "xxh64": L.ref_xxh64_u16(k, sd)} for k in keys16 for sd in (0, 1, 42)]
     return out
+
+
+def keys(L, rng):
+    """The reference's key comparison on floating-point bit patterns: EqualTo (==)
+    and the bitwise sentinel test, for fp16, float and double."""
+    specials = {
+        2: [0x0000, 0x8000, 0x3c00, 0xbc00, 0x7c00, 0xfc00, 0x7e00, 0x7c01, 0xfe00, 0x0001, 0x8001, 0x7bff],
+        4: [0x00000000, 0x80000000, 0x3f800000, 0xbf800000, 0x7f800000, 0xff800000, 0x7fc00000, 0x7f800001,
+            0xffc00000, 0x00000001, 0x80000001, 0x7f7fffff],
+        8: [0x0, 0x8000000000000000, 0x3ff0000000000000, 0xbff0000000000000, 0x7ff0000000000000,
+            0xfff0000000000000, 0x7ff8000000000000, 0x7ff0000000000001, 0xfff8000000000000, 0x1,
+            0x8000000000000001, 0x7fefffffffffffff],
+    }
+    fn = {2: L.ref_equal_f16, 4: L.ref_equal_f32, 8: L.ref_equal_f64}
+    rows = []
+    for kb, vals in specials.items():
+        for a in vals:
+            for b in vals:
+                rows.append({"key_bytes": kb, "a": a, "b": b, "equal": fn[kb](a, b, 0), "sentinel": fn[kb](a, b, 1)})
+    return {"float_key_comparisons": rows}
 
 
 def capacity(L, rng):
@@ -126,6 +159,17 @@ def probing(L, rng):
                             L.ref_probe_walk(kb, b, dh, hk, k, cap, 12, buf)
                             rows.append({"key_bytes": kb, "bucket_size": b, "double_hashing": dh, "hash": hk,
                                          "capacity": cap, "key": k, "walk": list(buf)})
+    r16 = np.random.default_rng(17)
+    for b in (1, 5, 8):
+        for dh in (0, 1):
+            for hk in (0, 1, 3):  # no Fmix for 2-byte keys
+                for cap_req in (40, 1000, 70_000):
+                    cap = L.ref_valid_capacity(cap_req, b, dh)
+                    for k in [0, 0xffff, 0x8000] + [int(x) for x in r16.integers(0, 1 << 16, size=3)]:
+                        buf = (C.c_uint32 * 12)()
+                        L.ref_probe_walk(2, b, dh, hk, k, cap, 12, buf)
+                        rows.append({"key_bytes": 2, "bucket_size": b, "double_hashing": dh, "hash": hk,
+                                     "capacity": cap, "key": k, "walk": list(buf)})
     return {"walks": rows}
 
 
@@ -216,12 +260,15 @@ def main():
     import sys
     sys.path.insert(0, REPO)
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("B2CO_REFERENCE")
+                    or os.path.join(os.path.dirname(REPO), "reference"))
     args = ap.parse_args()
+    if not os.path.isdir(os.path.join(args.ref, "include")):
+        ap.error(f"no reference checkout at {args.ref}: name it with --ref or B2CO_REFERENCE")
     L = load_probe(args.ref)
     rng = np.random.default_rng(2026)
     for name, fn in [("hashes", hashes), ("capacity", capacity), ("probing", probing), ("bloom", bloom),
-                     ("hll", hll), ("roaring", roaring)]:
+                     ("hll", hll), ("roaring", roaring), ("keys", keys)]:
         data = fn(L, rng)
         with open(os.path.join(HERE, f"{name}.json"), "w") as f:
             json.dump(data, f, separators=(",", ":"))

@@ -61,7 +61,7 @@ def test_create_validation_errors_before_any_device_work():
     L = b2co.lib()
     h = C.c_void_p()
     for kb, vb, b, pr, hs, res in [(3, 4, 5, 1, 0, 0), (4, 2, 5, 1, 0, 0), (4, 4, 3, 1, 0, 0), (4, 4, 5, 7, 0, 0),
-                                   (4, 4, 5, 1, 9, 0), (4, 4, 5, 1, 0, 1)]:
+                                   (4, 4, 5, 1, 9, 0), (4, 4, 5, 1, 0, 2)]:
         d = b2co.OaDesc(kb, vb, b, pr, hs, res, 0xffffffff, 0xffffffff, 0xffffffff)
         assert L.b2co_oa_create(C.byref(d), C.c_uint64(100), None, C.byref(h)) == b2co.EINVAL
         assert L.b2co_last_error()
@@ -120,3 +120,43 @@ def test_fastmod_is_exact():
         m = ((2**64 - 1) // d + 1) % 2**64
         for a in a_s:
             assert ((m * a % 2**64) * d) >> 64 == a % d, (a, d)
+
+
+def test_device_key_primitives_on_host_match_reference():
+    """The kernels' hash and key comparison (include/b2co/device.cuh), evaluated
+    on the host through the library, against the reference's own outputs."""
+    import json
+    L = b2co.lib()
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    g = json.load(open(os.path.join(here, "hashes.json")))
+    out = C.c_uint32()
+    for r in g["vectors16"]:
+        for hk, name in ((b2co.HASH_XXH32, "xxh32"), (b2co.HASH_MURMUR3_32, "murmur3_32"), (b2co.HASH_XXH64, "xxh64")):
+            assert L.b2co_probe_hash(hk, 2, C.c_uint64(r["key"]), r["seed"], C.byref(out)) == 0
+            assert out.value == r[name] & 0xFFFFFFFF, (name, r)
+    for r in g["vectors"][:200]:
+        for hk, name in ((b2co.HASH_XXH32, "xxh32"), (b2co.HASH_MURMUR3_32, "murmur3_32"), (b2co.HASH_XXH64, "xxh64"),
+                         (b2co.HASH_FMIX, "fmix")):
+            assert L.b2co_probe_hash(hk, r["key_bytes"], C.c_uint64(r["key"]), r["seed"], C.byref(out)) == 0
+            assert out.value == r[name] & 0xFFFFFFFF, (name, r)
+    assert L.b2co_probe_hash(b2co.HASH_FMIX, 2, C.c_uint64(1), 0, C.byref(out)) == b2co.EINVAL
+    eq = C.c_int()
+    for r in json.load(open(os.path.join(here, "keys.json")))["float_key_comparisons"]:
+        assert L.b2co_key_equal(1, r["key_bytes"], C.c_uint64(r["a"]), C.c_uint64(r["b"]), C.byref(eq)) == 0
+        assert eq.value == r["equal"], r
+        assert L.b2co_key_equal(0, r["key_bytes"], C.c_uint64(r["a"]), C.c_uint64(r["b"]), C.byref(eq)) == 0
+        assert eq.value == int(r["a"] == r["b"]), r
+
+
+def test_two_byte_and_float_layouts_validate():
+    """Descriptor checks of the new layouts, without touching the GPU."""
+    L = b2co.lib()
+    h = C.c_void_p()
+    for kb, vb, kind, hk in [(2, 4, 0, 0), (4, 2, 0, 0), (8, 2, 0, 0), (2, 8, 1, 0), (2, 0, 0, b2co.HASH_FMIX),
+                             (4, 4, 2, 0), (3, 0, 0, 0)]:
+        d = b2co.OaDesc(kb, vb, 5, 1, hk, kind, 0xFFFF, 0xFFFF, 0xFFFF)
+        assert L.b2co_oa_create(C.byref(d), C.c_uint64(100), None, C.byref(h)) == b2co.EINVAL, (kb, vb, kind, hk)
+    assert b2co.slot_bytes(2, 2) == 4 and b2co.slot_bytes(2, 0) == 2 and b2co.slot_bytes(4, 4) == 8
+    assert b2co.slot_bytes(4, 8) == 16 and b2co.slot_bytes(8, 4) == 16 and b2co.slot_bytes(8, 8) == 16
+    for kb, vb in [(2, 0), (2, 2), (4, 0), (4, 4), (4, 8), (8, 4), (8, 8)]:
+        assert oracle.slot_layout(kb, vb)[0] == b2co.slot_bytes(kb, vb)

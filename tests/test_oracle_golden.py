@@ -53,6 +53,31 @@ def test_hash_vectors_match_reference_headers():
         assert oracle.xxh64(kbytes(r["bits"], 4), r["seed"]) == r["h"]
 
 
+def test_two_byte_key_hashes_match_reference_headers():
+    """int16/uint16/fp16 keys hash their two bytes: XXH32 and XXH64 through their
+    single-byte tail steps, MurmurHash3 through its 2-byte tail (reference headers)."""
+    for r in load("hashes")["vectors16"]:
+        b = kbytes(r["key"], 2)
+        assert oracle.xxh32(b, r["seed"]) == r["xxh32"]
+        assert oracle.murmur3_32(b, r["seed"]) == r["murmur3_32"]
+        assert oracle.xxh64(b, r["seed"]) == r["xxh64"]
+
+
+def test_float_key_comparison_matches_reference():
+    """EqualTo on fp16 / float / double bit patterns (the reference's EqualWrapper
+    compiled here): -0 equals +0, NaN equals nothing.  The sentinel test is
+    bitwise for floating-point types (utility/traits.h:27-28); the host probe
+    stands in for fp16_t with _Float16, which this C++ library does not classify
+    as floating point, so its sentinel rows fall back to == and are not pinned."""
+    rows = load("keys")["float_key_comparisons"]
+    assert len(rows) == 3 * 144
+    for r in rows:
+        assert oracle.key_equal(oracle.KEY_FLOAT, r["key_bytes"], r["a"], r["b"]) == bool(r["equal"]), r
+        if r["key_bytes"] != 2:
+            assert bool(r["sentinel"]) == (r["a"] == r["b"]), r
+        assert oracle.key_equal(oracle.KEY_INT, r["key_bytes"], r["a"], r["b"]) == (r["a"] == r["b"])
+
+
 def test_prime_table_rule_reproduces_reference_table():
     g = load("capacity")
     t = oracle.prime_table().astype(np.int64)
