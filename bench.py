@@ -297,6 +297,8 @@ def run_gpu(args):
     found = torch.empty(stream_keys.numel(), dtype=torch.int64, device="cuda")
     inserted = torch.empty(stream_keys.numel(), dtype=torch.uint8, device="cuda")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # scratch for the largest fill this run times (LF 0.8), so no timed region allocates
+    t.ReserveInsertAndFind(sum(workload_sizes(cap, 0.8)))
     torch.cuda.synchronize()
     e0.record(stream)
     t.InsertAndFindAsync(pairs, found, inserted, mode=b2co.IAF_FIRST_WINS)
@@ -608,6 +610,7 @@ def insert_measurements(stream, capacity_log2=28, reps=3):
     found = torch.empty(unique, dtype=torch.int64, device="cuda")
     ins = torch.empty(unique, dtype=torch.uint8, device="cuda")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t.ReserveInsertAndFind(unique)
 
     def best(fn, clear=True):
         out = []
@@ -849,8 +852,10 @@ def batched_measurements(stream):
     e1.record(stream)
     torch.cuda.synchronize()
     res["batched_per_table_insert_gkeys"] = round(total / e0.elapsed_time(e1) / 1e6, 3)
-    lanes = grp.Autotune(q, d_q_off, ref)
-    res["batched_autotuned_lanes"] = lanes
+    b2co.tune_cache_clear()
+    shape, _ = grp.Autotune(q, d_q_off, ref)
+    res["batched_autotuned_shape"] = {"lanes": shape[0], "keys_per_tile": shape[1], "block": shape[2]}
+    res["batched_autotune_reused_from_cache"] = grp.Autotune(q, d_q_off, ref)[1]
     ms = timed(lambda: grp.Find(q, d_q_off, out))
     res["batched_group_find_gkeys"] = round(2 * total / ms / 1e6, 3)
     ms = timed(lambda: grp.Find(q, d_q_off, out, graph=True))
@@ -1204,12 +1209,21 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                 "copies": s1["copies"] - s0["copies"]}
 
     run_rate(rates[0], 128)  # warm-up: first launches of every table
-    out = []
+    out, plain = [], []
     for rate in rates:
         r = run_rate(rate, max(200, int(rate * seconds)))
         log(f"[served] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s, "
             f"{r['requests_per_launch']} req/launch, {r['host_us_per_launch']} us host/launch")
         out.append(r)
+    # the baseline on the same schedule: one plain launch per request, one
+    # request per table at a time (copy in, Find / InsertOrAssign, copy out)
+    srv.set_plain(True)
+    for rate in rates:
+        r = run_rate(rate, max(200, int(rate * seconds)))
+        log(f"[served plain] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s")
+        plain.append({k: r[k] for k in ("offered_req_s", "requests", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
+                                        "launches")})
+    srv.set_plain(False)
     st = srv.stats()
     srv.close()
     del tables
@@ -1219,7 +1233,8 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                        "request_pool": pool, "mean_request_keys": round(float(np.mean(ns)), 1),
                        "seconds_per_rate": seconds, "host_buffers": "pinned",
                        "staging_grows": st["staging_grows"], "max_loop_gap_us": round(st["max_loop_gap_ns"] / 1e3, 1),
-                       "sweep": out}}
+                       "sweep": out, "plain_per_table_sweep": plain,
+                       "server_over_plain_gkeys": [round(a["gkeys_s"] / b["gkeys_s"], 3) for a, b in zip(out, plain)]}}
 
 
 def run_reference(args):

@@ -174,6 +174,12 @@ int b2co_oa_insert_and_find(b2co_oa_table* table, const void* pairs, void* out_f
                             uint64_t n, int mode, b2co_stream stream);
 int b2co_oa_insert_and_find_async(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
                                   uint64_t n, int mode, b2co_stream stream);
+/* Sizes the library-owned scratch of first-wins InsertAndFind for batches of
+ * up to n items now (4 bytes per item, 4 + 1/8 bytes per slot), so later
+ * calls of at most n items allocate nothing and never wait on an allocation.
+ * Without it the scratch grows on first use.  No reference counterpart (the
+ * reference's InsertAndFind needs no scratch). */
+int b2co_oa_reserve_insert_and_find(b2co_oa_table* table, uint64_t n);
 /* First-wins InsertAndFind that allocates nothing, for callers that cannot
  * let a library allocate device memory (an application that owns all device
  * memory through its own arena under a fixed budget, or a latency-critical
@@ -282,12 +288,34 @@ int b2co_oa_group_find_per_table(b2co_oa_group* group, const void* keys, const u
                                  int contains, b2co_stream stream);
 int b2co_oa_group_insert_per_table(b2co_oa_group* group, const void* pairs, const uint64_t* h_offsets,
                                    b2co_stream stream);
-/* Lanes per key of the group Find (1, 2, 4 or 8). */
+/* Kernel shape of the group Find: lanes per bucket window (1, 2, 4 or 8),
+ * keys in flight per lane group (1, 2 or 4, at most the lanes; above 1 the
+ * keys whose first window settles nothing are queued and followed a pass at a
+ * time) and threads per block (64, 128 or 256; 0 = 256).  Results do not
+ * depend on it.  The default is 4 lanes, 2 keys, 256 threads.  The lanes-only
+ * form sets one key per lane group. */
 int b2co_oa_group_set_find_shape(b2co_oa_group* group, uint32_t lanes);
-/* Autotuner: times every lane count on this batch, keeps the fastest, and
- * leaves valid results in `out`. */
+int b2co_oa_group_set_find_shape_ex(b2co_oa_group* group, uint32_t lanes, uint32_t keys_per_tile, uint32_t block);
+int b2co_oa_group_get_find_shape(const b2co_oa_group* group, uint32_t* lanes, uint32_t* keys_per_tile,
+                                 uint32_t* block);
+/* Autotuner: times every group Find shape (lanes x keys per lane group x
+ * threads per block) on this batch, keeps the fastest, and leaves valid
+ * results in `out`.  The choice is cached under (operation, key bytes,
+ * payload bytes, bucket size, log2 of the mean table capacity) and a later
+ * call with the same key reuses it without timing (*from_cache = 1).  The
+ * cache lives in the process; b2co_tune_cache_save / _load write and read it
+ * as a text file, and a file named by the B2CO_TUNE_CACHE environment
+ * variable is loaded on first use and rewritten after every new result.  The
+ * lanes-only form reports the lanes of the chosen shape.  No reference
+ * counterpart (the batched pattern is this library's). */
+int b2co_oa_group_autotune(b2co_oa_group* group, const void* keys, const uint64_t* d_offsets, void* out, uint64_t n,
+                           b2co_stream stream, uint32_t* lanes, uint32_t* keys_per_tile, uint32_t* block,
+                           int* from_cache);
 int b2co_oa_group_autotune_find(b2co_oa_group* group, const void* keys, const uint64_t* d_offsets, void* out,
                                 uint64_t n, b2co_stream stream, uint32_t* chosen_lanes);
+int b2co_tune_cache_save(const char* path);
+int b2co_tune_cache_load(const char* path);
+int b2co_tune_cache_clear(void);
 
 /* ===================================================================== */
 /* Request server over resident tables                                      */
@@ -323,6 +351,12 @@ uint64_t b2co_server_now_ns(void);
 int b2co_server_create(uint32_t max_inflight, uint64_t hbm_budget_bytes, uint64_t max_batch_keys, b2co_server** out);
 /* Counts a resident table's bytes against the budget. */
 int b2co_server_register_table(b2co_server* server, b2co_oa_table* table);
+/* Plain mode (non-zero), the baseline the server is measured against: no
+ * coalescing, every request its own copy in, launch and copy out, and at most
+ * one request per table on the GPU at a time (a table's next request waits
+ * for the previous one to finish; different tables still overlap).  Set it
+ * while no request is queued. */
+int b2co_server_set_plain(b2co_server* server, int plain);
 /* host_in: keys (Find/Contains) or pairs (Insert/InsertOrAssign); host_out:
  * payloads (Find) or 1-byte flags (Contains), unused otherwise. */
 int b2co_server_submit(b2co_server* server, b2co_oa_table* table, int op, const void* host_in, void* host_out,

@@ -24,6 +24,7 @@
 #include <type_traits>
 #include <utility>
 
+#include <cuda_fp16.h>
 #include <cuda_runtime_api.h>
 
 #include "../b2co.h"
@@ -117,7 +118,15 @@ struct alignas(pair_alignment(sizeof(First) + sizeof(Second))) Pair {
     Second second;
 };
 
+// The reference's fp16_t key / payload type (2 bytes, IEEE binary16).
+using fp16_t = __half;
+
 namespace detail {
+
+// Floating-point keys (float, double, fp16_t) match with == in the reference
+// (EqualTo); the table is created with that key kind.
+template <typename T>
+constexpr bool is_float_key = std::is_floating_point<T>::value || std::is_same<T, __half>::value;
 
 template <typename T>
 uint64_t bits_of(T v)
@@ -158,6 +167,7 @@ class OpenAddressing {
         d.bucket_size = bucketSize;
         d.probing = ProbingScheme::probing;
         d.hash = ProbingScheme::hash;
+        d.key_kind = is_float_key<Key> ? B2CO_KEY_FLOAT : B2CO_KEY_INTEGER;
         d.empty_key_bits = bits_of(emptyKey);
         d.empty_value_bits = valueBytes ? bits_of(emptyValue) : 0;
         d.erased_key_bits = bits_of(erasedKey);
@@ -274,8 +284,9 @@ class OpenAddressing {
 template <class Key, class T, class ExtentT = Extent<std::size_t>, class KeyEqual = EqualTo<Key>,
           class ProbingScheme = LinearProbing<murmurhash3_32<Key>>, class StorageT = Storage<5>>
 class StaticMap : public detail::OpenAddressing<Key, T, ExtentT, KeyEqual, ProbingScheme, StorageT> {
-    static_assert(sizeof(Key) == 4 || sizeof(Key) == 8, "keys are 4 or 8 bytes");
-    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "payloads are 4 or 8 bytes");
+    static_assert(sizeof(Key) == 2 || sizeof(Key) == 4 || sizeof(Key) == 8, "keys are 2, 4 or 8 bytes");
+    static_assert(sizeof(Key) == 2 ? sizeof(T) == 2 : (sizeof(T) == 4 || sizeof(T) == 8),
+                  "2-byte keys take 2-byte payloads; wider keys take 4- or 8-byte payloads");
     using Base = detail::OpenAddressing<Key, T, ExtentT, KeyEqual, ProbingScheme, StorageT>;
 
    public:
@@ -334,7 +345,7 @@ class StaticMap : public detail::OpenAddressing<Key, T, ExtentT, KeyEqual, Probi
 template <class Key, class ExtentT = Extent<std::size_t>, class KeyEqual = EqualTo<Key>,
           class ProbingScheme = DoubleHashing<xxhash_32<Key>>, class StorageT = Storage<5>>
 class StaticSet : public detail::OpenAddressing<Key, Key, ExtentT, KeyEqual, ProbingScheme, StorageT> {
-    static_assert(sizeof(Key) == 4 || sizeof(Key) == 8, "keys are 4 or 8 bytes");
+    static_assert(sizeof(Key) == 2 || sizeof(Key) == 4 || sizeof(Key) == 8, "keys are 2, 4 or 8 bytes");
     using Base = detail::OpenAddressing<Key, Key, ExtentT, KeyEqual, ProbingScheme, StorageT>;
 
    public:
@@ -368,6 +379,10 @@ class StaticSet : public detail::OpenAddressing<Key, Key, ExtentT, KeyEqual, Pro
 template <class Key, class T, class ExtentT = Extent<std::size_t>, class KeyEqual = EqualTo<Key>,
           class ProbingScheme = LinearProbing<murmurhash3_32<Key>>, class StorageT = Storage<5>>
 class DynamicMap {
+    static_assert(!detail::is_float_key<Key> && (sizeof(Key) == 4 || sizeof(Key) == 8) &&
+                      (sizeof(T) == 4 || sizeof(T) == 8),
+                  "DynamicMap takes 4- or 8-byte integer keys and 4- or 8-byte payloads");
+
    public:
     using SizeType = typename ExtentT::ValueType;
     enum class InsertMode { kExactDedup, kAppendUnique };

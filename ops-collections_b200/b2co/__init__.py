@@ -348,6 +348,10 @@ class _OaBase:
             (FIND_WARP_STAGED if warp_staged else 0) | (FIND_DEFERRED if deferred else 0)
         _call("b2co_oa_set_find_shape", self._h, C.c_uint32(lanes_per_key), C.c_uint32(keys_per_lane | flags))
 
+    def ReserveInsertAndFind(self, n: int):
+        """Size first-wins InsertAndFind's scratch for batches up to n now (b2co_oa_reserve_insert_and_find)."""
+        _call("b2co_oa_reserve_insert_and_find", self._h, C.c_uint64(n))
+
     def set_write_shape(self, lanes_per_key: int, keys_per_tile: int):
         """Kernel shape of the insert family (b2co_oa_set_write_shape); (0, 0) = default."""
         _call("b2co_oa_set_write_shape", self._h, C.c_uint32(lanes_per_key), C.c_uint32(keys_per_tile))
@@ -474,14 +478,23 @@ class TableGroup:
         h = np.ascontiguousarray(h_offsets, dtype=np.uint64)
         _call("b2co_oa_group_insert_per_table", self._h, _ptr(pairs), C.c_void_p(h.ctypes.data), _stream(stream))
 
-    def set_find_shape(self, lanes):
-        _call("b2co_oa_group_set_find_shape", self._h, C.c_uint32(lanes))
+    def set_find_shape(self, lanes, keys_per_tile=1, block=0):
+        _call("b2co_oa_group_set_find_shape_ex", self._h, C.c_uint32(lanes), C.c_uint32(keys_per_tile),
+              C.c_uint32(block))
 
-    def Autotune(self, keys, d_offsets, out, stream=None) -> int:
-        v = C.c_uint32()
-        _call("b2co_oa_group_autotune_find", self._h, _ptr(keys), _ptr(d_offsets), _ptr(out),
-              C.c_uint64(keys.shape[0]), _stream(stream), C.byref(v))
-        return v.value
+    def find_shape(self):
+        """(lanes, keys per lane group, threads per block) of the group Find."""
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _call("b2co_oa_group_get_find_shape", self._h, C.byref(a), C.byref(b), C.byref(c))
+        return a.value, b.value, c.value
+
+    def Autotune(self, keys, d_offsets, out, stream=None):
+        """Times every group Find shape on this batch (or reuses the cached
+        choice); returns ((lanes, keys per lane group, block), from_cache)."""
+        a, b, c, hit = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_int()
+        _call("b2co_oa_group_autotune", self._h, _ptr(keys), _ptr(d_offsets), _ptr(out), C.c_uint64(keys.shape[0]),
+              _stream(stream), C.byref(a), C.byref(b), C.byref(c), C.byref(hit))
+        return (a.value, b.value, c.value), bool(hit.value)
 
 
 OP_FIND, OP_CONTAINS, OP_INSERT, OP_INSERT_OR_ASSIGN = 0, 1, 2, 3
@@ -529,6 +542,10 @@ class Server:
 
     def register(self, table):
         _call("b2co_server_register_table", self._h, table._h)
+
+    def set_plain(self, plain: bool):
+        """Plain mode: one launch per request, one request per table at a time (the baseline)."""
+        _call("b2co_server_set_plain", self._h, C.c_int(1 if plain else 0))
 
     def submit(self, table, op, host_in: np.ndarray, host_out=None, arrival_ns: int = 0) -> int:
         """Queues a request; the arrays are kept alive until wait() returns."""
@@ -1009,6 +1026,18 @@ class HyperLogLog:
         h = np.zeros(65, dtype=np.uint32)
         _call("b2co_hll_histogram", self._h, _stream(stream), C.c_void_p(h.ctypes.data))
         return h
+
+
+def tune_cache_save(path: str):
+    _call("b2co_tune_cache_save", path.encode())
+
+
+def tune_cache_load(path: str):
+    _call("b2co_tune_cache_load", path.encode())
+
+
+def tune_cache_clear():
+    _call("b2co_tune_cache_clear")
 
 
 def hll_finalize(precision: int, hist) -> int:

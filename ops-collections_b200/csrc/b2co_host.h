@@ -91,7 +91,8 @@ struct GroupArgs;
 
 // Launchers of the persistent group kernels for one slot layout.
 struct GroupOps {
-    int (*find)(GroupArgs const& g, uint32_t b, uint32_t lanes, bool contains, void const* keys, void* out,
+    // shape: lanes | keys per lane group << 8 | threads per block << 16
+    int (*find)(GroupArgs const& g, uint32_t b, uint32_t shape, bool contains, void const* keys, void* out,
                 uint64_t n, cudaStream_t s);
     int (*insert)(GroupArgs const& g, uint32_t b, void const* pairs, uint64_t n, unsigned long long* failed,
                   cudaStream_t s);

@@ -7,9 +7,15 @@
 // array of per-table descriptors, and runs each operation over all tables in
 // one launch -- optionally replayed from a CUDA graph -- instead of one launch
 // per table.  The per-table launch path is kept as the baseline to beat.
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <string>
+#include <tuple>
 #include <vector>
 
 #include "b2co_host.h"
@@ -29,7 +35,7 @@ struct b2co_oa_group {
     GroupTable* d_tables = nullptr;
     unsigned long long* d_counters = nullptr;  // [failed, status]
     unsigned long long* h_counters = nullptr;
-    uint32_t find_lanes = 2;
+    uint32_t find_shape = 4u | (2u << 8);  // lanes | keys per lane group << 8 | block << 16 (0 = 256)
     // one cached graph of the group Find launch
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -37,7 +43,7 @@ struct b2co_oa_group {
     void const* g_offsets = nullptr;
     void* g_out = nullptr;
     uint64_t g_n = 0;
-    uint32_t g_lanes = 0;
+    uint32_t g_shape = 0;
     bool g_contains = false;
 };
 
@@ -72,7 +78,7 @@ GroupArgs group_args(b2co_oa_group const* g, uint64_t const* d_offsets)
 
 OaArgs table_args(b2co_oa_group const* g, uint32_t t)
 {
-    OaArgs a;
+    OaArgs a{};
     a.slots = static_cast<char*>(g->slab) + g->host_tables[t].slot_offset * g->slot_bytes;
     a.probe = g->host_tables[t].probe;
     a.empty_key = g->desc.empty_key_bits;
@@ -85,6 +91,96 @@ int check(b2co_oa_group const* g)
 {
     if (!g || !g->slab) return fail(B2CO_ELOGIC, "table group is null or has no storage");
     return B2CO_OK;
+}
+
+// ---- autotune cache ----------------------------------------------------------
+// Keyed by (op, key bytes, payload bytes, bucket size, capacity bucket); the
+// value is a packed kernel shape and the time it measured.
+struct TuneKey {
+    uint32_t op, kb, vb, b, cap_bucket;
+    bool operator<(TuneKey const& o) const
+    {
+        return std::tie(op, kb, vb, b, cap_bucket) < std::tie(o.op, o.kb, o.vb, o.b, o.cap_bucket);
+    }
+};
+struct TuneVal {
+    uint32_t shape;
+    float ms;
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+bool g_tune_env_loaded = false;
+
+uint32_t capacity_bucket(uint64_t mean_capacity)
+{
+    uint32_t b = 0;
+    while (mean_capacity > 1) mean_capacity >>= 1, ++b;
+    return b;
+}
+
+int load_file_locked(char const* path)
+{
+    FILE* f = std::fopen(path, "r");
+    if (!f) return fail(B2CO_EINVAL, std::string("cannot read the tune cache ") + path);
+    char line[256];
+    while (std::fgets(line, sizeof line, f)) {
+        char op[32];
+        TuneKey k{};
+        unsigned lanes, items, block;
+        float ms;
+        if (std::sscanf(line, "%31s %u %u %u %u %u %u %u %f", op, &k.kb, &k.vb, &k.b, &k.cap_bucket, &lanes, &items,
+                        &block, &ms) != 9 || std::strcmp(op, "group_find") != 0)
+            continue;  // comments and unknown operations
+        g_tune[k] = TuneVal{lanes | (items << 8) | (block << 16), ms};
+    }
+    std::fclose(f);
+    return B2CO_OK;
+}
+
+int save_file_locked(char const* path)
+{
+    FILE* f = std::fopen(path, "w");
+    if (!f) return fail(B2CO_EINVAL, std::string("cannot write the tune cache ") + path);
+    std::fprintf(f, "# op key_bytes payload_bytes bucket log2_capacity lanes keys_per_tile block ms\n");
+    for (auto const& kv : g_tune) {
+        TuneKey const& k = kv.first;
+        uint32_t const sh = kv.second.shape;
+        std::fprintf(f, "group_find %u %u %u %u %u %u %u %.4f\n", k.kb, k.vb, k.b, k.cap_bucket, sh & 0xffu,
+                     (sh >> 8) & 0xffu, (sh >> 16) ? (sh >> 16) : 256u, kv.second.ms);
+    }
+    std::fclose(f);
+    return B2CO_OK;
+}
+
+void env_load_locked()
+{
+    if (g_tune_env_loaded) return;
+    g_tune_env_loaded = true;
+    if (char const* p = std::getenv("B2CO_TUNE_CACHE")) {
+        if (FILE* f = std::fopen(p, "r")) {
+            std::fclose(f);
+            load_file_locked(p);
+        }
+    }
+}
+
+bool tune_cache_get(TuneKey const& k, uint32_t* shape)
+{
+    std::lock_guard<std::mutex> l(g_tune_mu);
+    env_load_locked();
+    auto it = g_tune.find(k);
+    if (it == g_tune.end()) return false;
+    *shape = it->second.shape;
+    return true;
+}
+
+void tune_cache_put(TuneKey const& k, uint32_t shape, float ms)
+{
+    std::lock_guard<std::mutex> l(g_tune_mu);
+    env_load_locked();
+    g_tune[k] = TuneVal{shape, ms};
+    if (char const* p = std::getenv("B2CO_TUNE_CACHE")) save_file_locked(p);
 }
 
 }  // namespace
@@ -223,7 +319,7 @@ int b2co_oa_group_find(b2co_oa_group* g, void const* keys, uint64_t const* d_off
     if (int st = check(g)) return st;
     if (n == 0 || !keys || !out) return B2CO_OK;
     if (!d_offsets) return fail(B2CO_EINVAL, "offsets must not be null");
-    return g->gops->find(group_args(g, d_offsets), g->desc.bucket_size, g->find_lanes, contains != 0, keys, out, n,
+    return g->gops->find(group_args(g, d_offsets), g->desc.bucket_size, g->find_shape, contains != 0, keys, out, n,
                          cs(s));
 }
 
@@ -236,14 +332,14 @@ int b2co_oa_group_find_graph(b2co_oa_group* g, void const* keys, uint64_t const*
     if (n == 0 || !keys || !out) return B2CO_OK;
     if (!d_offsets) return fail(B2CO_EINVAL, "offsets must not be null");
     bool const same = g->graph && g->g_keys == keys && g->g_offsets == d_offsets && g->g_out == out && g->g_n == n &&
-                      g->g_lanes == g->find_lanes && g->g_contains == (contains != 0);
+                      g->g_shape == g->find_shape && g->g_contains == (contains != 0);
     if (!same) {
         if (g->graph) {
             cudaGraphExecDestroy(g->graph);
             g->graph = nullptr;
         }
         B2CO_CUDA(cudaStreamBeginCapture(g->capture_stream, cudaStreamCaptureModeThreadLocal));
-        int st = g->gops->find(group_args(g, d_offsets), g->desc.bucket_size, g->find_lanes, contains != 0, keys, out,
+        int st = g->gops->find(group_args(g, d_offsets), g->desc.bucket_size, g->find_shape, contains != 0, keys, out,
                                n, g->capture_stream);
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(g->capture_stream, &graph);
@@ -259,7 +355,7 @@ int b2co_oa_group_find_graph(b2co_oa_group* g, void const* keys, uint64_t const*
         g->g_offsets = d_offsets;
         g->g_out = out;
         g->g_n = n;
-        g->g_lanes = g->find_lanes;
+        g->g_shape = g->find_shape;
         g->g_contains = contains != 0;
     }
     B2CO_CUDA(cudaGraphLaunch(g->graph, cs(s)));
@@ -298,44 +394,123 @@ int b2co_oa_group_insert_per_table(b2co_oa_group* g, void const* pairs, uint64_t
     return B2CO_OK;
 }
 
-int b2co_oa_group_set_find_shape(b2co_oa_group* g, uint32_t lanes)
+int b2co_oa_group_set_find_shape_ex(b2co_oa_group* g, uint32_t lanes, uint32_t keys_per_tile, uint32_t block)
 {
     if (int st = check(g)) return st;
     if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) return fail(B2CO_EINVAL, "lanes must be 1, 2, 4 or 8");
-    g->find_lanes = lanes;
+    if (keys_per_tile != 1 && keys_per_tile != 2 && keys_per_tile != 4)
+        return fail(B2CO_EINVAL, "keys per lane group must be 1, 2 or 4");
+    if (keys_per_tile > lanes && lanes > 1) return fail(B2CO_EINVAL, "keys per lane group cannot exceed the lanes");
+    if (block != 0 && block != 64 && block != 128 && block != 256)
+        return fail(B2CO_EINVAL, "threads per block must be 64, 128 or 256");
+    g->find_shape = lanes | (keys_per_tile << 8) | (block << 16);
     return B2CO_OK;
 }
 
-// Autotuner: times the group Find with every lane count on the caller's own
-// batch and keeps the fastest.  Outputs are overwritten with valid results.
-int b2co_oa_group_autotune_find(b2co_oa_group* g, void const* keys, uint64_t const* d_offsets, void* out, uint64_t n,
-                                b2co_stream s, uint32_t* chosen_lanes)
+int b2co_oa_group_set_find_shape(b2co_oa_group* g, uint32_t lanes)
+{
+    return b2co_oa_group_set_find_shape_ex(g, lanes, 1, 0);
+}
+
+int b2co_oa_group_get_find_shape(b2co_oa_group const* g, uint32_t* lanes, uint32_t* keys_per_tile, uint32_t* block)
+{
+    if (int st = check(g)) return st;
+    if (lanes) *lanes = g->find_shape & 0xffu;
+    if (keys_per_tile) *keys_per_tile = (g->find_shape >> 8) & 0xffu;
+    if (block) *block = (g->find_shape >> 16) ? (g->find_shape >> 16) : 256u;
+    return B2CO_OK;
+}
+
+// Autotuner: times the group Find with every kernel shape -- lanes per window,
+// keys in flight per lane group, threads per block -- on the caller's own
+// batch and keeps the fastest.  Results are cached in the process under (op,
+// key bytes, payload bytes, bucket size, log2 of the mean table capacity) and
+// reused without timing; the cache can be saved to and loaded from a file
+// (b2co_tune_cache_save / _load, or the B2CO_TUNE_CACHE file, loaded on first
+// use and rewritten after each new result).  Outputs are overwritten with
+// valid results.
+int b2co_oa_group_autotune(b2co_oa_group* g, void const* keys, uint64_t const* d_offsets, void* out, uint64_t n,
+                           b2co_stream s, uint32_t* lanes, uint32_t* keys_per_tile, uint32_t* block, int* from_cache)
 {
     if (int st = check(g)) return st;
     if (n == 0 || !keys || !out || !d_offsets) return fail(B2CO_EINVAL, "autotune needs a non-empty batch");
-    cudaStream_t c = cs(s);
-    cudaEvent_t e0, e1;
-    B2CO_CUDA(cudaEventCreate(&e0));
-    B2CO_CUDA(cudaEventCreate(&e1));
-    float best = 1e30f;
-    uint32_t best_lanes = g->find_lanes;
-    for (uint32_t lanes : {1u, 2u, 4u, 8u}) {
-        g->find_lanes = lanes;
-        if (int st = b2co_oa_group_find(g, keys, d_offsets, out, n, 0, s)) return st;  // warm
-        B2CO_CUDA(cudaEventRecord(e0, c));
-        for (int r = 0; r < 3; ++r)
-            if (int st = b2co_oa_group_find(g, keys, d_offsets, out, n, 0, s)) return st;
-        B2CO_CUDA(cudaEventRecord(e1, c));
-        B2CO_CUDA(cudaEventSynchronize(e1));
-        float ms = 0;
-        B2CO_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best) best = ms, best_lanes = lanes;
+    TuneKey const key{0, g->desc.key_bytes, g->desc.value_bytes, g->desc.bucket_size,
+                      capacity_bucket(g->total_slots / g->count)};
+    uint32_t shape = 0;
+    bool const hit = tune_cache_get(key, &shape);
+    if (!hit) {
+        cudaStream_t c = cs(s);
+        cudaEvent_t e0, e1;
+        B2CO_CUDA(cudaEventCreate(&e0));
+        B2CO_CUDA(cudaEventCreate(&e1));
+        float best = 1e30f;
+        uint32_t const saved = g->find_shape;
+        shape = saved;
+        static uint32_t const kLanes[] = {1, 2, 4, 8}, kItems[] = {1, 2, 4}, kBlocks[] = {128, 256};
+        int st = B2CO_OK;
+        for (uint32_t ln : kLanes) {
+            for (uint32_t it : kItems) {
+                if ((ln == 1 && it > 1) || (ln > 1 && it > ln)) continue;
+                for (uint32_t bl : kBlocks) {
+                    g->find_shape = ln | (it << 8) | (bl << 16);
+                    if ((st = b2co_oa_group_find(g, keys, d_offsets, out, n, 0, s))) break;  // warm
+                    cudaEventRecord(e0, c);
+                    for (int r = 0; r < 3 && !st; ++r) st = b2co_oa_group_find(g, keys, d_offsets, out, n, 0, s);
+                    cudaEventRecord(e1, c);
+                    cudaEventSynchronize(e1);
+                    float ms = 0;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (st) break;
+                    if (ms < best) best = ms, shape = g->find_shape;
+                }
+                if (st) break;
+            }
+            if (st) break;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st) {
+            g->find_shape = saved;
+            return st;
+        }
+        tune_cache_put(key, shape, best / 3.0f);
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    g->find_lanes = best_lanes;
-    if (chosen_lanes) *chosen_lanes = best_lanes;
+    g->find_shape = shape;
+    if (from_cache) *from_cache = hit ? 1 : 0;
+    b2co_oa_group_get_find_shape(g, lanes, keys_per_tile, block);
     return b2co_oa_group_find(g, keys, d_offsets, out, n, 0, s);
+}
+
+// The lanes-only form of the autotuner (the shape it picks is kept whole).
+int b2co_oa_group_autotune_find(b2co_oa_group* g, void const* keys, uint64_t const* d_offsets, void* out, uint64_t n,
+                                b2co_stream s, uint32_t* chosen_lanes)
+{
+    return b2co_oa_group_autotune(g, keys, d_offsets, out, n, s, chosen_lanes, nullptr, nullptr, nullptr);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int b2co_tune_cache_save(char const* path)
+{
+    if (!path) return fail(B2CO_EINVAL, "null path");
+    std::lock_guard<std::mutex> l(g_tune_mu);
+    return save_file_locked(path);
+}
+
+int b2co_tune_cache_load(char const* path)
+{
+    if (!path) return fail(B2CO_EINVAL, "null path");
+    std::lock_guard<std::mutex> l(g_tune_mu);
+    return load_file_locked(path);
+}
+
+int b2co_tune_cache_clear(void)
+{
+    std::lock_guard<std::mutex> l(g_tune_mu);
+    g_tune.clear();
+    return B2CO_OK;
 }
 
 }  // extern "C"

@@ -106,6 +106,143 @@ __global__ void __launch_bounds__(256) k_group_find(GroupArgs g, void const* key
     }
 }
 
+// The group lookup in the single-table default's shape: G lanes share a
+// window, each tile keeps Q keys in flight, and a key whose first window
+// settles nothing is queued in the warp's shared-memory ring with its table
+// and followed a pass at a time (a pass waits on one window load).  Each
+// q-slot of a tile walks forward through the tables on its own, so a pass may
+// span a table boundary.  Blocks of up to 256 threads.
+template <class S, int B, int G, int Q, bool CONTAINS>
+__global__ void __launch_bounds__(256) k_group_find_q(GroupArgs g, void const* keys, void* out, uint64_t n)
+{
+    static_assert(Q <= G && G >= 2 && G <= 8, "tile shape");
+    using Raw = typename S::Raw;
+    constexpr int ROUNDS = (B + G - 1) / G;
+    constexpr uint32_t TILES = 32 / G;
+    constexpr uint32_t PASS = TILES * Q;
+    static_assert(2 * PASS <= kDeferRing, "the ring must hold a pass on top of a partial one");
+    constexpr uint32_t RING = kDeferRing - 1;
+    __shared__ uint64_t qkey[8][kDeferRing], qpos[8][kDeferRing];
+    __shared__ uint32_t qtab[8][kDeferRing], qinit[8][kDeferRing], qidx[8][kDeferRing];
+
+    uint32_t const lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t const r = lane % G, tile_lane0 = lane & ~uint32_t(G - 1), tile = lane / G;
+    uint64_t begin, end;
+    warp_span(n, PASS, begin, end);
+    if (begin >= end) return;  // warp-uniform
+    uint32_t head = 0, count = 0;
+    using Key = typename Io<S>::Key;
+    Key const* kin = static_cast<Key const*>(keys);
+
+    auto write = [&](uint64_t pos, bool hit, Raw const& slot, uint64_t empty) {
+        if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[pos] = hit;
+        else reinterpret_cast<typename Io<S>::Payload*>(out)[pos] = typename Io<S>::Payload(hit ? S::value(slot) : empty);
+    };
+    auto enqueue = [&](bool unsettled, uint64_t key, uint32_t tab, uint32_t init, uint32_t idx, uint64_t pos) {
+        uint32_t const m = __ballot_sync(0xffffffffu, unsettled);
+        if (unsettled) {
+            uint32_t const e = (head + count + __popc(m & ((1u << lane) - 1u))) & RING;
+            qkey[warp][e] = key;
+            qtab[warp][e] = tab;
+            qinit[warp][e] = init;
+            qidx[warp][e] = idx;
+            qpos[warp][e] = pos;
+        }
+        count += __popc(m);
+    };
+    uint64_t const empty = S::is_set ? g.empty_key : g.empty_value;
+    auto follow = [&]() {
+        __syncwarp();
+        uint32_t const take = count < PASS ? count : PASS;
+        uint64_t key[Q], pos[Q];
+        uint32_t tab[Q], init[Q], idx[Q];
+        bool live[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t const j = q * TILES + tile;
+            live[q] = j < take;
+            uint32_t const e = (head + (live[q] ? j : 0u)) & RING;
+            key[q] = qkey[warp][e];
+            tab[q] = qtab[warp][e];
+            init[q] = qinit[warp][e];
+            idx[q] = qidx[warp][e];
+            pos[q] = qpos[warp][e];
+        }
+        __syncwarp();
+        head = (head + take) & RING;
+        count -= take;
+        Raw w[Q][ROUNDS];
+        Raw const* base[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            GroupTable const& T = g.tables[live[q] ? tab[q] : 0u];
+            base[q] = static_cast<Raw const*>(g.slots) + T.slot_offset;
+            if (live[q]) {
+                idx[q] = probe_next(idx[q], probe_step<S::key_bytes, B>(T.probe, key[q]), T.probe.capacity);
+                if (idx[q] == init[q]) {  // a whole cycle: not present
+                    if (r == 0) write(pos[q], false, Raw{}, empty);
+                    live[q] = false;
+                }
+            }
+            load_range<S, B, G, ROUNDS>(base[q], idx[q], 0, B, r, !live[q], w[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            int own;
+            Raw mine{};
+            int const st = tile_first_stop<S, B, G, ROUNDS>(w[q], !live[q], key[q], g.empty_key, r, own, mine);
+            if (live[q] && st != kNoStop && own == st) write(pos[q], S::key(mine) != g.empty_key, mine, empty);
+            enqueue(live[q] && st == kNoStop && r == 0, key[q], tab[q], init[q], idx[q], pos[q]);
+        }
+    };
+
+    uint32_t tq[Q];
+    uint64_t nextq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        uint64_t const i = begin + q * TILES + tile;
+        tq[q] = group_table_of(g.offsets, g.count, i < end ? i : end - 1);
+        nextq[q] = __ldg(g.offsets + tq[q] + 1);
+    }
+    for (uint64_t i0 = begin; i0 < end; i0 += PASS) {
+        uint64_t key[Q];
+        uint32_t idx[Q];
+        bool live[Q];
+        uint32_t my_init = 0;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint64_t const i = i0 + q * TILES + tile;
+            live[q] = i < end;
+            if (live[q] && i >= nextq[q]) {
+                do {
+                    ++tq[q];
+                    nextq[q] = __ldg(g.offsets + tq[q] + 1);
+                } while (i >= nextq[q]);
+            }
+            key[q] = live[q] ? uint64_t(__ldg(kin + i)) : 0;
+            if (int(r) == q && live[q]) my_init = probe_init<S::key_bytes, B>(g.tables[tq[q]].probe, key[q]);
+        }
+        Raw w[Q][ROUNDS];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            idx[q] = __shfl_sync(0xffffffffu, my_init, tile_lane0 + q);
+            Raw const* base = static_cast<Raw const*>(g.slots) + g.tables[tq[q]].slot_offset;
+            load_range<S, B, G, ROUNDS>(base, idx[q], 0, B, r, !live[q], w[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            int own;
+            Raw mine{};
+            uint64_t const i = i0 + q * TILES + tile;
+            int const st = tile_first_stop<S, B, G, ROUNDS>(w[q], !live[q], key[q], g.empty_key, r, own, mine);
+            if (live[q] && st != kNoStop && own == st) write(i, S::key(mine) != g.empty_key, mine, empty);
+            enqueue(live[q] && st == kNoStop && r == 0, key[q], tq[q], idx[q], idx[q], i);
+        }
+        while (count >= PASS) follow();
+    }
+    while (count > 0) follow();
+}
+
 template <class S, int B>
 __global__ void __launch_bounds__(256) k_group_insert(GroupArgs g, void const* pairs, uint64_t n,
                                                       unsigned long long* failed_counter)

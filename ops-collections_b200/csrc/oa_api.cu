@@ -495,6 +495,13 @@ int b2co_oa_insert_and_find_async(b2co_oa_table* t, void const* pairs, void* out
                              t->d_newbits, t->d_owner, cs(s));
 }
 
+int b2co_oa_reserve_insert_and_find(b2co_oa_table* t, uint64_t n)
+{
+    if (int st = check_table(t)) return st;
+    if (int st = check_batch(n)) return st;
+    return ensure_first_wins_scratch(t, n ? n : 1);
+}
+
 int b2co_oa_insert_and_find(b2co_oa_table* t, void const* pairs, void* out_found, uint8_t* out_inserted, uint64_t n,
                             int mode, b2co_stream s)
 {

@@ -259,7 +259,11 @@ struct OaImpl {
     {
         bool const stageable = !stencil && (reinterpret_cast<uintptr_t>(keys) & 15) == 0 && n >= kStageKeys && B > 1;
         // bulk-window path: 16-byte slots only
-        if ((items & kShapeBulk) && stageable && S::bytes == 16) return find_bulk<B, C>(a, keys, out, n, wc, s);
+        if constexpr (B == 5) {  // the block-staged, warp-staged and bulk shapes: bucket size 5 only (build time)
+            if ((items & kShapeBulk) && stageable && S::bytes == 16) return find_bulk<B, C>(a, keys, out, n, wc, s);
+        } else if (stageable && lanes >= 2) {
+            items |= kShapeDeferred;  // other bucket sizes stage keys the default way
+        }
         items &= ~kShapeBulk;
         // staged path: no stencil, 16-byte aligned key stream, at least one stage of keys
         bool const staged = stageable && lanes >= 2;
@@ -270,25 +274,28 @@ struct OaImpl {
             return find_wdefer<B, 8, C>(a, items, keys, out, n, wc, s);
         }
         items &= ~kShapeDeferred;
-        if (staged && (items & kShapeWarpStaged)) {
-            items &= ~(kShapeWarpStaged | kShapeSegmented);
-            if (lanes == 2) return find_wstaged<B, 2, C>(a, items, keys, out, n, wc, s);
-            if (lanes == 4) return find_wstaged<B, 4, C>(a, items, keys, out, n, wc, s);
-            return find_wstaged<B, 8, C>(a, items, keys, out, n, wc, s);
+        if constexpr (B == 5) {
+            if (staged && (items & kShapeWarpStaged)) {
+                items &= ~(kShapeWarpStaged | kShapeSegmented);
+                if (lanes == 2) return find_wstaged<B, 2, C>(a, items, keys, out, n, wc, s);
+                if (lanes == 4) return find_wstaged<B, 4, C>(a, items, keys, out, n, wc, s);
+                return find_wstaged<B, 8, C>(a, items, keys, out, n, wc, s);
+            }
+            items &= ~kShapeWarpStaged;
+            if (staged) {
+                bool const seg = (items & kShapeSegmented) != 0;
+                items &= ~kShapeSegmented;
+                if (seg) {
+                    if (lanes == 2) return find_staged<B, 2, C, true>(a, items, keys, out, n, wc, s);
+                    if (lanes == 4) return find_staged<B, 4, C, true>(a, items, keys, out, n, wc, s);
+                    return find_staged<B, 8, C, true>(a, items, keys, out, n, wc, s);
+                }
+                if (lanes == 2) return find_staged<B, 2, C, false>(a, items, keys, out, n, wc, s);
+                if (lanes == 4) return find_staged<B, 4, C, false>(a, items, keys, out, n, wc, s);
+                return find_staged<B, 8, C, false>(a, items, keys, out, n, wc, s);
+            }
         }
         items &= ~kShapeWarpStaged;
-        if (staged) {
-            bool const seg = (items & kShapeSegmented) != 0;
-            items &= ~kShapeSegmented;
-            if (seg) {
-                if (lanes == 2) return find_staged<B, 2, C, true>(a, items, keys, out, n, wc, s);
-                if (lanes == 4) return find_staged<B, 4, C, true>(a, items, keys, out, n, wc, s);
-                return find_staged<B, 8, C, true>(a, items, keys, out, n, wc, s);
-            }
-            if (lanes == 2) return find_staged<B, 2, C, false>(a, items, keys, out, n, wc, s);
-            if (lanes == 4) return find_staged<B, 4, C, false>(a, items, keys, out, n, wc, s);
-            return find_staged<B, 8, C, false>(a, items, keys, out, n, wc, s);
-        }
         items &= ~kShapeSegmented;
         void (*k)(OaArgs, void const*, uint8_t const*, void*, uint32_t) = nullptr;
         uint64_t per_block = kBlock;
@@ -346,25 +353,43 @@ template <class S>
 struct GroupImpl {
     static constexpr uint32_t kBlock = 256;
 
+    // `shape` packs lanes per window (bits 0-7), keys in flight per lane group
+    // (bits 8-15; 1 = one key per tile, resolved at once) and threads per block
+    // (bits 16-31; 0 = 256).  Keys per tile above 1 run the deferred kernel;
+    // its 2-, 4- and 8-lane variants other than 4x2 exist for bucket size 5.
     template <int B, bool C>
-    static int find_b(GroupArgs const& g, uint32_t lanes, void const* keys, void* out, uint64_t n, cudaStream_t s)
+    static int find_b(GroupArgs const& g, uint32_t shape, void const* keys, void* out, uint64_t n, cudaStream_t s)
     {
+        uint32_t const lanes = shape & 0xffu, items = (shape >> 8) & 0xffu;
+        uint32_t const block = (shape >> 16) ? (shape >> 16) : kBlock;
         void (*k)(GroupArgs, void const*, void*, uint64_t) = nullptr;
-        if (lanes <= 1) k = k_group_find<S, B, 1, C>;
-        else if (lanes == 2) k = k_group_find<S, B, 2, C>;
-        else if (lanes == 4) k = k_group_find<S, B, 4, C>;
-        else k = k_group_find<S, B, 8, C>;
+        if (lanes >= 2 && items >= 2) {
+            if constexpr (B == 5) {
+                if (lanes == 2) k = k_group_find_q<S, B, 2, 2, C>;
+                else if (lanes == 4 && items >= 4) k = k_group_find_q<S, B, 4, 4, C>;
+                else if (lanes == 8) k = items >= 4 ? k_group_find_q<S, B, 8, 4, C> : k_group_find_q<S, B, 8, 2, C>;
+            }
+            if (!k) k = k_group_find_q<S, B, 4, 2, C>;
+        } else if (lanes <= 1) {
+            k = k_group_find<S, B, 1, C>;
+        } else if (lanes == 2) {
+            k = k_group_find<S, B, 2, C>;
+        } else if (lanes == 4) {
+            k = k_group_find<S, B, 4, C>;
+        } else {
+            k = k_group_find<S, B, 8, C>;
+        }
         // persistent: every resident block, spans balanced by items
-        k<<<grid_for((void const*)k, kBlock, n, 1), kBlock, 0, s>>>(g, keys, out, n);
+        k<<<grid_for((void const*)k, block, n, 1), block, 0, s>>>(g, keys, out, n);
         return OaImpl<S>::check_launch(C ? "group contains kernel" : "group find kernel");
     }
 
-    static int find(GroupArgs const& g, uint32_t b, uint32_t lanes, bool contains, void const* keys, void* out,
+    static int find(GroupArgs const& g, uint32_t b, uint32_t shape, bool contains, void const* keys, void* out,
                     uint64_t n, cudaStream_t s)
     {
         return OaImpl<S>::with_b(b, [&](auto bc) {
             constexpr int B = decltype(bc)::value;
-            return contains ? find_b<B, true>(g, lanes, keys, out, n, s) : find_b<B, false>(g, lanes, keys, out, n, s);
+            return contains ? find_b<B, true>(g, shape, keys, out, n, s) : find_b<B, false>(g, shape, keys, out, n, s);
         });
     }
 

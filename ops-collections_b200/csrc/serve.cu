@@ -91,6 +91,10 @@ enum class Fit { kOk, kWait, kNever, kError };
 struct b2co_server {
     int device = 0;
     uint64_t budget = 0, max_batch_keys = 0;
+    // plain mode: every request is its own launch and a table has at most one
+    // launch in flight (copy in, kernel, copy out, then the table's next
+    // request); the baseline the coalescing server is measured against
+    std::atomic<bool> plain{false};
 
     // submission side (in_mu)
     std::mutex in_mu;
@@ -293,9 +297,56 @@ struct b2co_server {
         cv_done.notify_all();
     }
 
+    // Plain mode's admission: the earliest arrived request of each table that
+    // has no launch in flight, alone, in arrival order per table (tables run
+    // side by side on the slots).
+    bool admit_plain()
+    {
+        bool progress = false;
+        uint64_t const t = now_ns();
+        while (!queue.empty() && queue.front()->taken) queue.pop_front();
+        std::vector<b2co_oa_table const*> blocked;
+        for (auto& sl : slots)
+            if (sl.busy) blocked.push_back(sl.reqs.front()->table);
+        size_t const scan = std::min<size_t>(queue.size(), kCoalesceScan);
+        for (size_t i = 0; i < scan; ++i) {
+            Request* r = queue[i];
+            if (r->taken) continue;
+            if (r->info.arrival_ns > t) break;
+            if (std::find(blocked.begin(), blocked.end(), r->table) != blocked.end()) continue;
+            blocked.push_back(r->table);  // the table's later requests wait for this one
+            std::vector<Request*> g{r};
+            Slot* sl = pick_slot(staging_bytes(g));
+            if (!sl) return progress;
+            Fit const fit = reserve(*sl, staging_bytes(g));
+            if (fit == Fit::kWait) return progress;
+            if (fit != Fit::kOk) {
+                r->taken = true;
+                finish({r}, fit == Fit::kNever ? B2CO_ENOMEM : B2CO_ECUDA, t);
+                progress = true;
+                continue;
+            }
+            r->taken = true;
+            r->info.admit_ns = t;
+            uint64_t const l0 = now_ns();
+            int const st = launch(*sl, g);
+            uint64_t const dl = now_ns() - l0;
+            raise_max(max_launch_ns, dl);
+            launch_ns += dl;
+            if (st) {
+                cudaStreamSynchronize(sl->stream);
+                cudaGetLastError();
+                finish(g, st, now_ns());
+            }
+            progress = true;
+        }
+        return progress;
+    }
+
     // Admits what the slots and the budget allow; true if anything changed.
     bool admit()
     {
+        if (plain.load(std::memory_order_relaxed)) return admit_plain();
         bool progress = false;
         uint64_t const t = now_ns();
         for (;;) {
@@ -522,6 +573,13 @@ int b2co_server_create(uint32_t max_inflight, uint64_t hbm_budget_bytes, uint64_
     }
     s->worker = std::thread([s] { s->run(); });
     *out = guard.release();
+    return B2CO_OK;
+}
+
+int b2co_server_set_plain(b2co_server* s, int plain)
+{
+    if (!s) return fail(B2CO_EINVAL, "null server");
+    s->plain.store(plain != 0);
     return B2CO_OK;
 }
 

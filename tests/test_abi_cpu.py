@@ -160,3 +160,23 @@ def test_two_byte_and_float_layouts_validate():
     assert b2co.slot_bytes(4, 8) == 16 and b2co.slot_bytes(8, 4) == 16 and b2co.slot_bytes(8, 8) == 16
     for kb, vb in [(2, 0), (2, 2), (4, 0), (4, 4), (4, 8), (8, 4), (8, 8)]:
         assert oracle.slot_layout(kb, vb)[0] == b2co.slot_bytes(kb, vb)
+
+
+def test_tune_cache_file_round_trip(tmp_path):
+    """The batched pattern's autotune cache persists as a text file: entries
+    load, unknown lines and comments are skipped, and a save writes them back."""
+    src = tmp_path / "in.txt"
+    src.write_text("# op key_bytes payload_bytes bucket log2_capacity lanes keys_per_tile block ms\n"
+                   "group_find 4 4 5 15 4 2 256 1.2500\nsomething_else 1 2 3\n"
+                   "group_find 8 8 5 20 8 4 128 3.0000\n")
+    b2co.tune_cache_clear()
+    b2co.tune_cache_load(str(src))
+    dst = tmp_path / "out.txt"
+    b2co.tune_cache_save(str(dst))
+    rows = [ln for ln in dst.read_text().splitlines() if not ln.startswith("#")]
+    assert rows == ["group_find 4 4 5 15 4 2 256 1.2500", "group_find 8 8 5 20 8 4 128 3.0000"]
+    b2co.tune_cache_clear()
+    b2co.tune_cache_save(str(dst))
+    assert [ln for ln in dst.read_text().splitlines() if not ln.startswith("#")] == []
+    with pytest.raises(b2co.InvalidArgument):
+        b2co.tune_cache_load(str(tmp_path / "missing.txt"))

@@ -31,7 +31,7 @@ def build_workload(rng, count):
     return sizes, keys, vals, queries, ins_off, q_off
 
 
-def test_group_insert_find_graph_per_table_match_oracle():
+def test_group_insert_find_graph_per_table_match_oracle(tmp_path):
     import b2co
     import torch
     rng = np.random.default_rng(404)
@@ -60,12 +60,17 @@ def test_group_insert_find_graph_per_table_match_oracle():
 
     qd = dev(qcat)
     d_qoff = dev(q_off.astype(np.int64))
-    for lanes in (1, 2, 4, 8):
-        g.set_find_shape(lanes)
+    shapes = [(1, 1, 0), (2, 1, 0), (4, 1, 0), (8, 1, 0), (2, 2, 256), (4, 2, 0), (4, 4, 128), (8, 2, 256),
+              (8, 4, 64)]
+    for shape in shapes:  # every shape, deferred or not, block sizes included
+        g.set_find_shape(*shape)
         out = torch.empty(len(qcat), dtype=torch.int32, device="cuda")
         g.Find(qd, d_qoff, out)
         torch.cuda.synchronize()
-        assert np.array_equal(out.cpu().numpy(), expected), lanes
+        assert np.array_equal(out.cpu().numpy(), expected), shape
+        c = torch.empty(len(qcat), dtype=torch.uint8, device="cuda")
+        g.Find(qd, d_qoff, c, contains=True)
+        assert np.array_equal(c.cpu().numpy(), (expected != -1).astype(np.uint8)), shape
     out = torch.empty(len(qcat), dtype=torch.int32, device="cuda")
     g.Find(qd, d_qoff, out, graph=True)
     g.Find(qd, d_qoff, out, graph=True)  # replay
@@ -79,10 +84,21 @@ def test_group_insert_find_graph_per_table_match_oracle():
     g.Find(qd, d_qoff, c, contains=True)
     torch.cuda.synchronize()
     assert np.array_equal(c.cpu().numpy(), (expected != -1).astype(np.uint8))
+    b2co.tune_cache_clear()
     out = torch.empty(len(qcat), dtype=torch.int32, device="cuda")
-    lanes = g.Autotune(qd, d_qoff, out)
-    assert lanes in (1, 2, 4, 8)
+    shape, cached = g.Autotune(qd, d_qoff, out)
+    assert not cached and shape[0] in (1, 2, 4, 8) and shape == g.find_shape()
     assert np.array_equal(out.cpu().numpy(), expected)
+    # the choice is reused without timing, and survives a save / clear / load round trip
+    out = torch.empty(len(qcat), dtype=torch.int32, device="cuda")
+    assert g.Autotune(qd, d_qoff, out) == (shape, True)
+    assert np.array_equal(out.cpu().numpy(), expected)
+    path = str(tmp_path / "tune.txt")
+    b2co.tune_cache_save(path)
+    b2co.tune_cache_clear()
+    b2co.tune_cache_load(path)
+    g.set_find_shape(1)
+    assert g.Autotune(qd, d_qoff, out) == (shape, True) and g.find_shape() == shape
 
     # the per-table insert path builds the same tables
     g2 = b2co.TableGroup(caps, -1, -1, key_dtype=torch.int32, value_dtype=torch.int32)
