@@ -591,7 +591,10 @@ def extra_measurements(t, keys, q50, out, stream, args):
     return res
 
 
-def insert_measurements(stream, capacity_log2=28, reps=3):
+INSERT_SHAPES = [(1, 1), (2, 1), (2, 2), (4, 1), (4, 2), (4, 4), (8, 2), (8, 4)]
+
+
+def insert_measurements(stream, capacity_log2=28, reps=3, shapes=None):
     """The write side of the headline table on its own: StaticMap<int64,int64>,
     DoubleHashing<xxhash_32>, bucket 5, requested capacity 2^capacity_log2; a
     cleared table filled to LF 0.5 by Insert (unique keys), by InsertAndFind in
@@ -635,6 +638,13 @@ def insert_measurements(stream, capacity_log2=28, reps=3):
     res["first_wins_exact"] = bool(int(ins.sum().item()) == unique) and bool(torch.equal(found, vals))
     ms = best(lambda: t.InsertOrAssignAsync(pairs, stream=stream), clear=False)
     res["insert_or_assign_dup_gkeys"] = round(unique / ms / 1e6, 3)
+    if shapes:  # Insert with every write-kernel shape (lanes per window x keys per lane group)
+        sweep = {}
+        for lanes, items in shapes:
+            t.set_write_shape(lanes, items)
+            sweep[f"{lanes}x{items}"] = round(unique / best(lambda: t.InsertAsync(pairs, stream=stream)) / 1e6, 3)
+        t.set_write_shape(0, 0)
+        res["insert_shape_sweep_gkeys"] = sweep
     del t
     return res
 
@@ -949,6 +959,18 @@ def bloom_part(f_time, g, peak):
     ms = time_once(lambda: f.AddAsync(adds))
     res["bloom_add_gkeys"] = round(n / ms / 1e6, 3)
     res["bloom_add_hbm_frac"] = round(n * 72 / (ms / 1e3) / 1e9 / peak, 4)
+    # the same Add through TMA bulk reductions (one 32-byte OR per key); same bits
+    atomic_words = f.words()
+    f.set_add_mode(b2co.BLOOM_ADD_BULK)
+    f.Clear()
+    f.AddAsync(adds)
+    f.Clear()
+    ms = time_once(lambda: f.AddAsync(adds))
+    res["bloom_add_bulk_gkeys"] = round(n / ms / 1e6, 3)
+    res["bloom_add_bulk_hbm_frac"] = round(n * 72 / (ms / 1e3) / 1e9 / peak, 4)
+    res["bloom_add_bulk_equals_atomic"] = bool(np.array_equal(f.words(), atomic_words))
+    del atomic_words
+    f.set_add_mode(b2co.BLOOM_ADD_ATOMIC)
     out = torch.empty(q.numel(), dtype=torch.uint8, device="cuda")
     f.ContainsAsync(q, out)
     ms = time_once(lambda: f.ContainsAsync(q, out))
@@ -956,7 +978,7 @@ def bloom_part(f_time, g, peak):
     res["bloom_contains_hbm_frac"] = round(q.numel() * 41 / (ms / 1e3) / 1e9 / peak, 4)
     res["bloom_no_false_negatives"] = bool(out[: n // 2].all().item())
     res["bloom_false_positive_rate"] = round(float(out[n // 2:].float().mean().item()), 6)
-    del adds, absent, q, out, f
+    del adds, q, out, f
     return res
 
 
@@ -1310,7 +1332,8 @@ def main():
               "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2),
               "multi": multi_measurements, "roaring": roaring_measurements,
               "small_map": small_map_measurements, "dmap": dynamic_map_measurements,
-              "insert": lambda st: insert_measurements(st, capacity_log2=args.capacity_log2)}[args.only]
+              "insert": lambda st: insert_measurements(st, capacity_log2=args.capacity_log2,
+                                                       shapes=INSERT_SHAPES if args.sweep else None)}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
         run_reference(args)

@@ -175,7 +175,7 @@ int b2co_oa_insert_and_find(b2co_oa_table* table, const void* pairs, void* out_f
 int b2co_oa_insert_and_find_async(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
                                   uint64_t n, int mode, b2co_stream stream);
 /* Sizes the library-owned scratch of first-wins InsertAndFind for batches of
- * up to n items now (4 bytes per item, 4 + 1/8 bytes per slot), so later
+ * up to n items now (4 bytes per item, 4 + 1/4 bytes per slot), so later
  * calls of at most n items allocate nothing and never wait on an allocation.
  * Without it the scratch grows on first use.  No reference counterpart (the
  * reference's InsertAndFind needs no scratch). */
@@ -185,7 +185,7 @@ int b2co_oa_reserve_insert_and_find(b2co_oa_table* table, uint64_t n);
  * memory through its own arena under a fixed budget, or a latency-critical
  * path that must not pay for a device allocation).  No counterpart in the
  * reference.  Same results as b2co_oa_insert_and_find(..., B2CO_IAF_FIRST_WINS)
- * and synchronous like it, but the scratch (4 bytes per item, 4 + 1/8 bytes
+ * and synchronous like it, but the scratch (4 bytes per item, 4 + 1/4 bytes
  * per table slot) comes from a fixed 32 MiB device array inside the library,
  * which every GPU that loads the library holds until the process exits.
  * Batches needing more scratch fail with B2CO_ERANGE.  Every call looks up
@@ -530,6 +530,14 @@ int b2co_bloom_clear_async(b2co_bloom* filter, b2co_stream stream);
 /* reference: bloom_filter.h:69-72 Add / AddAsync / AddIf / AddIfAsync
  * (bloom_filter_impl.h:40-47, bloom_filter_add.inl:15-89). */
 int b2co_bloom_add(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream stream);
+/* How Add of the default policy (8 words per block, one bit per word) updates
+ * the filter; the bits set are the same either way.  B2CO_BLOOM_ADD_ATOMIC:
+ * four 64-bit atomic ORs per key from the SM.  B2CO_BLOOM_ADD_BULK: one
+ * 32-byte TMA bulk reduction (OR) per key from shared memory.  No reference
+ * counterpart (the reference chooses between atomics and a routed path by
+ * batch size, bloom_filter_launch.inl:131-240). */
+typedef enum { B2CO_BLOOM_ADD_ATOMIC = 0, B2CO_BLOOM_ADD_BULK = 1 } b2co_bloom_add_mode;
+int b2co_bloom_set_add_mode(b2co_bloom* filter, int mode);
 int b2co_bloom_add_async(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream stream);
 int b2co_bloom_add_if(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint64_t n, b2co_stream stream);
 int b2co_bloom_add_if_async(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint64_t n,

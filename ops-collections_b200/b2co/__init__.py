@@ -35,6 +35,7 @@ FIND_SEGMENTED = 0x100
 FIND_BULK = 0x200
 FIND_WARP_STAGED = 0x400
 FIND_DEFERRED = 0x800
+BLOOM_ADD_ATOMIC, BLOOM_ADD_BULK = 0, 1
 
 
 class B2coError(Exception):
@@ -916,6 +917,10 @@ class BloomFilter:
         p = C.c_void_p()
         _call("b2co_bloom_data", self._h, C.byref(p))
         return p.value
+
+    def set_add_mode(self, mode: int):
+        """BLOOM_ADD_ATOMIC (64-bit atomics) or BLOOM_ADD_BULK (TMA bulk OR) for the default policy's Add."""
+        _call("b2co_bloom_set_add_mode", self._h, C.c_int(mode))
 
     def words(self) -> np.ndarray:
         """The filter's words copied to the host (uint32, words_per_block per block)."""

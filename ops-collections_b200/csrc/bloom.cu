@@ -82,6 +82,41 @@ __global__ void __launch_bounds__(256) k_bloom_add(uint32_t* words, uint32_t nbl
     }
 }
 
+// Bulk-reduction Add (default policy): every key writes its block's eight
+// words (one bit each) to its own 32-byte slot in shared memory and the TMA
+// unit ORs the whole 32-byte block into the filter with one
+// cp.reduce.async.bulk .or.b32 (element-wise atomic in L2), instead of four
+// 64-bit atomics from the SM.  Each thread double-buffers its slot: before
+// reusing a slot it waits until the bulk operation that read it has read it.
+template <int KB>
+__global__ void __launch_bounds__(256) k_bloom_add_bulk(uint32_t* words, uint32_t nblocks, uint64_t seed,
+                                                        void const* keys, uint8_t const* stencil, uint64_t n)
+{
+    __shared__ alignas(128) uint32_t stage[2][256][8];
+    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
+    uint32_t b = 0;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (stencil && !stencil[i]) continue;
+        uint32_t block, lower;
+        locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower);
+        // the bulk operation issued two keys ago read this slot: wait for that read
+        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+        uint32_t* slot = stage[b][threadIdx.x];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            reinterpret_cast<uint4*>(slot)[q] = make_uint4(word_bit(4 * q, lower), word_bit(4 * q + 1, lower),
+                                                           word_bit(4 * q + 2, lower), word_bit(4 * q + 3, lower));
+        fence_proxy_async();  // the generic-proxy writes above precede the bulk read
+        asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.or.b32 [%0], [%1], 32;" ::"l"(
+                         words + uint64_t(block) * 8),
+                     "r"(smem_u32(slot))
+                     : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        b ^= 1u;
+    }
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // every reduction done before the slots go away
+}
+
 template <int KB>
 __global__ void __launch_bounds__(256) k_bloom_contains(uint32_t const* words, uint32_t nblocks, uint64_t seed,
                                                         void const* keys, uint8_t const* stencil, uint8_t* out,
@@ -208,6 +243,7 @@ cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 
 struct b2co_bloom {
     uint32_t* words = nullptr;
+    int add_mode = B2CO_BLOOM_ADD_ATOMIC;  // default-policy Add: 64-bit atomics or bulk reductions
     uint64_t num_blocks = 0;
     uint32_t key_bytes = 0;
     uint64_t seed = 0;
@@ -284,8 +320,9 @@ int add_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_s
         return fail(B2CO_EINVAL, "BloomFilter::AddIf: stencil must not be null when keyNum is non-zero");
     if (!f->default_policy())
         return f->key_bytes == 8 ? launch_add_policy<8>(f, keys, stencil, n, s) : launch_add_policy<4>(f, keys, stencil, n, s);
-    void (*k)(uint32_t*, uint32_t, uint64_t, void const*, uint8_t const*, uint64_t) =
-        f->key_bytes == 8 ? k_bloom_add<8> : k_bloom_add<4>;
+    void (*k)(uint32_t*, uint32_t, uint64_t, void const*, uint8_t const*, uint64_t) = nullptr;
+    if (f->add_mode == B2CO_BLOOM_ADD_BULK) k = f->key_bytes == 8 ? k_bloom_add_bulk<8> : k_bloom_add_bulk<4>;
+    else k = f->key_bytes == 8 ? k_bloom_add<8> : k_bloom_add<4>;
     k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks), f->seed, keys, stencil,
                                                            n);
     B2CO_CUDA(cudaGetLastError());
@@ -491,6 +528,18 @@ int b2co_bloom_intersect(b2co_bloom* f, b2co_bloom const* o, b2co_stream s)
 {
     if (int st = combine<1>(f, o, cs(s), "Intersect")) return st;
     return sync(cs(s));
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int b2co_bloom_set_add_mode(b2co_bloom* f, int mode)
+{
+    if (int st = check(f)) return st;
+    if (mode != B2CO_BLOOM_ADD_ATOMIC && mode != B2CO_BLOOM_ADD_BULK) return fail(B2CO_EINVAL, "unknown Add mode");
+    f->add_mode = mode;
+    return B2CO_OK;
 }
 
 }  // extern "C"

@@ -57,12 +57,12 @@ int b2co_oa_insert_and_find_noalloc(b2co_oa_table* t, void const* pairs, void* o
     if (n == 0 || !pairs) return B2CO_OK;
     if (!out_found || !out_inserted) return b2co::fail(B2CO_EINVAL, "InsertAndFind outputs must not be null");
     size_t const pos_bytes = align256(n * 4);
-    size_t const bits_bytes = align256(((capacity + 31) / 32) * 4);
+    size_t const bits_bytes = align256(((capacity + 31) / 32) * 8);  // two bitmaps of the slots
     size_t const owner_bytes = align256(capacity * 4);
     size_t const need = pos_bytes + bits_bytes + owner_bytes;
     if (n > b2co::kMaxBatch || need > kNoAllocScratchBytes)
         return b2co::fail(B2CO_ERANGE, "no-alloc InsertAndFind needs " + std::to_string(need) +
-                                           " bytes of scratch (4 per item, 4 per slot, 1/8 per slot); the static "
+                                           " bytes of scratch (4 per item, 4 per slot, 1/4 per slot); the static "
                                            "area holds " + std::to_string(kNoAllocScratchBytes));
     void* base = nullptr;
     if (int st = scratch_address(&base)) return st;

@@ -145,7 +145,7 @@ int ensure_first_wins_scratch(b2co_oa_table* t, uint64_t n)
 {
     if (!t->d_newbits) {
         uint64_t words = (t->capacity + 31) / 32;
-        B2CO_CUDA(cudaMalloc(&t->d_newbits, words * 4));
+        B2CO_CUDA(cudaMalloc(&t->d_newbits, 2 * words * 4));  // claimed bits, then lowered bits
         B2CO_CUDA(cudaMalloc(&t->d_owner, t->capacity * 4));
     }
     if (t->pos_cap < n) {
@@ -167,7 +167,7 @@ int b2co_oa_iaf_first_wins_on(b2co_oa_table* t, void const* pairs, void* out_fou
 {
     if (int st = check_table(t)) return st;
     if (int st = check_batch(n)) return st;
-    B2CO_CUDA(cudaMemsetAsync(newbits, 0, ((t->capacity + 31) / 32) * 4, s));
+    B2CO_CUDA(cudaMemsetAsync(newbits, 0, ((t->capacity + 31) / 32) * 8, s));
     return t->ops->iaf_first(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), pos, newbits,
                              owner, s);
 }
@@ -490,7 +490,7 @@ int b2co_oa_insert_and_find_async(b2co_oa_table* t, void const* pairs, void* out
         return t->ops->iaf_race(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), cs(s));
     if (mode != B2CO_IAF_FIRST_WINS) return fail(B2CO_EINVAL, "unknown InsertAndFind mode");
     if (int st = ensure_first_wins_scratch(t, n)) return st;
-    B2CO_CUDA(cudaMemsetAsync(t->d_newbits, 0, ((t->capacity + 31) / 32) * 4, cs(s)));
+    B2CO_CUDA(cudaMemsetAsync(t->d_newbits, 0, ((t->capacity + 31) / 32) * 8, cs(s)));
     return t->ops->iaf_first(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), t->d_pos,
                              t->d_newbits, t->d_owner, cs(s));
 }

@@ -42,6 +42,7 @@ struct InsOut {
     uint32_t* pos;                 // place: slot of every input (kNoSlot = failed)
     uint32_t* newbits;             // place: slots claimed by this batch
     uint32_t* owner;               // place: claiming input of each claimed slot
+    uint32_t claim_bit;            // place: flag OR-ed into pos[] of the claiming input (0 = none)
 };
 
 // Coherent window loads (L2, never a stale L1 line) with the 64-byte fill hint.
@@ -72,92 +73,119 @@ __device__ __forceinline__ unsigned short ld_win(unsigned short const* p)
 
 enum { kWinOpen = 0, kWinSettled = 1, kWinIdle = 2, kWinExhausted = 3 };
 
-// One bucket window of one key per tile, resolved cooperatively (the whole
-// warp calls it; tiles whose state is not kWinOpen only take part in the
-// shuffles).  On return a tile's state is kWinSettled (verdict, slot and, for
+// Resolution of the bucket windows of the Q keys each tile has in flight (the
+// whole warp calls it; tiles whose state is not kWinOpen only take part in the
+// shuffles).  On return a key's state is kWinSettled (verdict, slot and, for
 // the race mode, the found payload set on every lane of the tile) or
-// kWinExhausted (no slot of the window decided: probe on).
-template <class S, int B, int G, int ROUNDS, int MODE>
-__device__ __forceinline__ void tile_insert_window(OaArgs const& a, typename S::Raw* win_base,
-                                                   typename S::Raw (&w)[ROUNDS], uint64_t key, uint64_t val,
-                                                   uint32_t r, uint32_t lane0, int& state, int& verdict, int& slot,
-                                                   uint64_t& found)
+// kWinExhausted (no slot of the window decided: probe on).  The first deciding
+// slot of every key is found, then the CASes of all Q keys are issued back to
+// back before any result is awaited, so a pass waits on one CAS round trip
+// instead of Q.  A lost CAS updates the snapshot with the winner; a torn read
+// retries the slot; a slot that keeps changing (not seen in practice) gives
+// the rest of the window up after a bounded number of rounds.
+template <class S, int B, int G, int Q, int ROUNDS, int MODE>
+__device__ __forceinline__ void tile_insert_windows(OaArgs const& a, typename S::Raw* const (&win_base)[Q],
+                                                    typename S::Raw (&w)[Q][ROUNDS], uint64_t const (&key)[Q],
+                                                    uint64_t const (&val)[Q], uint32_t r, uint32_t lane0,
+                                                    int (&state)[Q], int (&verdict)[Q], int (&slot)[Q],
+                                                    uint64_t (&found)[Q])
 {
     using Raw = typename S::Raw;
-    uint32_t skip = 0;  // window slots ruled out without changing the snapshot
+    uint32_t skip[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) skip[q] = 0;
     for (int guard = 0; guard < 4 * B + 8; ++guard) {
-        if (!__any_sync(0xffffffffu, state == kWinOpen)) return;
-        int own = kNoStop;
-        Raw mine{};
-        if (state == kWinOpen) {
+        bool open = false;
 #pragma unroll
-            for (int t = ROUNDS - 1; t >= 0; --t) {
-                int const j = int(r) + t * G;
-                if (j < B && !((skip >> j) & 1u)) {
-                    uint64_t const k = S::key(w[t]);
-                    if (k == a.empty_key || S::key_eq(k, key)) {
-                        own = j;
-                        mine = w[t];
+        for (int q = 0; q < Q; ++q) open = open || state[q] == kWinOpen;
+        if (!__any_sync(0xffffffffu, open)) return;
+        int s[Q], own[Q], outcome[Q];
+        Raw mine[Q], old[Q];
+        uint64_t got[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            own[q] = kNoStop;
+            mine[q] = Raw{};
+            if (state[q] == kWinOpen) {
+#pragma unroll
+                for (int t = ROUNDS - 1; t >= 0; --t) {
+                    int const j = int(r) + t * G;
+                    if (j < B && !((skip[q] >> j) & 1u)) {
+                        uint64_t const k = S::key(w[q][t]);
+                        if (k == a.empty_key || S::key_eq(k, key[q])) {
+                            own[q] = j;
+                            mine[q] = w[q][t];
+                        }
                     }
                 }
             }
-        }
-        int s = own;
+            s[q] = own[q];
 #pragma unroll
-        for (int o = 1; o < G; o <<= 1) s = min(s, __shfl_xor_sync(0xffffffffu, s, o));
-        // outcome decided by the lane holding slot s: 1 inserted, 2 duplicate,
-        // 3 lost to another key (snapshot updated), 4 lost to a torn read
-        // (snapshot updated, retry the slot), 5 skip the slot
-        int outcome = 0;
-        uint64_t got = 0;
-        if (state == kWinOpen && s != kNoStop && own == s) {
-            Raw* sp = win_base + s;
-            uint64_t const k = S::key(mine);
-            if (k != a.empty_key) {
-                outcome = 2;
-                if constexpr (MODE == kInsAssign) assign_payload<S>(sp, key, val);
-                if constexpr (MODE == kInsIafRace) got = S::value(settle<S>(a, sp, mine));
-            } else {
-                Raw expected;
-                if (!insert_expected<S>(a, mine, expected)) {
-                    outcome = 5;
+            for (int o = 1; o < G; o <<= 1) s[q] = min(s[q], __shfl_xor_sync(0xffffffffu, s[q], o));
+        }
+        // issue: every key's deciding lane starts its CAS (or settles a duplicate)
+        Raw expected[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            outcome[q] = 0;
+            got[q] = 0;
+            if (state[q] == kWinOpen && s[q] != kNoStop && own[q] == s[q]) {
+                Raw* sp = win_base[q] + s[q];
+                if (S::key(mine[q]) != a.empty_key) {
+                    outcome[q] = 2;
+                    if constexpr (MODE == kInsAssign) assign_payload<S>(sp, key[q], val[q]);
+                    if constexpr (MODE == kInsIafRace) got[q] = S::value(settle<S>(a, sp, mine[q]));
+                } else if (!insert_expected<S>(a, mine[q], expected[q])) {
+                    outcome[q] = 5;
                 } else {
-                    Raw const old = cas_slot(sp, expected, insert_desired<S>(mine, key, val));
-                    if (raw_eq(old, expected)) {
-                        outcome = 1;
-                        got = S::is_set ? key : val;
-                    } else if (S::key_eq(S::key(old), key)) {
-                        outcome = 2;
-                        if constexpr (MODE == kInsAssign) assign_payload<S>(sp, key, val);
-                        got = S::value(old);
-                    } else {
-                        outcome = S::key(old) == a.empty_key ? 4 : 3;
-                    }
-#pragma unroll
-                    for (int t = 0; t < ROUNDS; ++t)
-                        if (int(r) + t * G == s) w[t] = old;
+                    outcome[q] = -1;  // CAS in flight
+                    old[q] = cas_slot(sp, expected[q], insert_desired<S>(mine[q], key[q], val[q]));
                 }
             }
         }
-        int const src = int(lane0) + (s == kNoStop ? 0 : s % G);
-        outcome = __shfl_sync(0xffffffffu, outcome, src);
-        if constexpr (MODE == kInsIafRace) got = __shfl_sync(0xffffffffu, (unsigned long long)got, src);
-        if (state == kWinOpen) {
-            if (s == kNoStop) {
-                state = kWinExhausted;
-            } else if (outcome == 1 || outcome == 2) {
-                state = kWinSettled;
-                verdict = outcome == 1 ? kSuccess : kDuplicate;
-                slot = s;
-                found = got;
-            } else if (outcome == 5) {
-                skip |= 1u << s;
+        // settle the CASes
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (outcome[q] == -1) {
+                Raw* sp = win_base[q] + s[q];
+                if (raw_eq(old[q], expected[q])) {
+                    outcome[q] = 1;
+                    got[q] = S::is_set ? key[q] : val[q];
+                } else if (S::key_eq(S::key(old[q]), key[q])) {
+                    outcome[q] = 2;
+                    if constexpr (MODE == kInsAssign) assign_payload<S>(sp, key[q], val[q]);
+                    got[q] = S::value(old[q]);
+                } else {
+                    outcome[q] = S::key(old[q]) == a.empty_key ? 4 : 3;
+                }
+#pragma unroll
+                for (int t = 0; t < ROUNDS; ++t)
+                    if (int(r) + t * G == s[q]) w[q][t] = old[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            int const src = int(lane0) + (s[q] == kNoStop ? 0 : s[q] % G);
+            int const oc = __shfl_sync(0xffffffffu, outcome[q], src);
+            uint64_t g = 0;
+            if constexpr (MODE == kInsIafRace) g = __shfl_sync(0xffffffffu, (unsigned long long)got[q], src);
+            if (state[q] == kWinOpen) {
+                if (s[q] == kNoStop) {
+                    state[q] = kWinExhausted;
+                } else if (oc == 1 || oc == 2) {
+                    state[q] = kWinSettled;
+                    verdict[q] = oc == 1 ? kSuccess : kDuplicate;
+                    slot[q] = s[q];
+                    found[q] = g;
+                } else if (oc == 5) {
+                    skip[q] |= 1u << s[q];
+                }
             }
         }
     }
-    // a slot that keeps changing under a torn read (not seen in practice):
-    // give the rest of the window up, the next window continues the probe
-    if (state == kWinOpen) state = kWinExhausted;
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        if (state[q] == kWinOpen) state[q] = kWinExhausted;
 }
 
 template <class S, int B, int G, int Q, int MODE>
@@ -198,7 +226,7 @@ __global__ void __launch_bounds__(256, 4) k_insert_win(__grid_constant__ const O
                 atomicOr(o.newbits + (p >> 5), 1u << (p & 31));
                 o.owner[p] = i;
             }
-            o.pos[i] = p;
+            o.pos[i] = verdict == kSuccess ? (p | o.claim_bit) : p;
         }
         (void)key;
     };
@@ -256,18 +284,41 @@ __global__ void __launch_bounds__(256, 4) k_insert_win(__grid_constant__ const O
                     if (int(r) + t * G < B) w[q][t] = ld_win(slots + idx[q] + r + t * G);
             }
         }
+        {
+            Raw* base[Q];
+            uint64_t key[Q], val[Q], found[Q];
+            int verdict[Q], slot[Q];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            int verdict = kFailed, slot = 0;
-            uint64_t found = 0;
-            uint64_t const key = S::key(pr[q]);
-            tile_insert_window<S, B, G, ROUNDS, MODE>(a, slots + idx[q], w[q], key, S::value(pr[q]), r, tile_lane0,
-                                                      state[q], verdict, slot, found);
-            if (state[q] == kWinSettled && r == 0) record(pos[q], verdict, idx[q] + slot, key, found);
-            enqueue(state[q] == kWinExhausted && r == 0, pr[q], init[q], idx[q], pos[q]);
+            for (int q = 0; q < Q; ++q) {
+                base[q] = slots + idx[q];
+                key[q] = S::key(pr[q]);
+                val[q] = S::value(pr[q]);
+                verdict[q] = kFailed;
+                slot[q] = 0;
+                found[q] = 0;
+            }
+            tile_insert_windows<S, B, G, Q, ROUNDS, MODE>(a, base, w, key, val, r, tile_lane0, state, verdict, slot,
+                                                          found);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                if (state[q] == kWinSettled && r == 0) record(pos[q], verdict[q], idx[q] + slot[q], key[q], found[q]);
+                enqueue(state[q] == kWinExhausted && r == 0, pr[q], init[q], idx[q], pos[q]);
+            }
         }
     };
 
+    // the next pass's pairs are loaded one pass ahead
+    Raw nxt[Q];
+    bool nin[Q];
+    auto load_pass = [&](uint32_t base) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            uint32_t const i = base + q * TILES + tile;
+            nin[q] = i < n && (!stencil || stencil[i]);
+            nxt[q] = nin[q] ? Io<S>::load_pair(pairs, i) : Raw{};
+        }
+    };
+    load_pass(gwarp * PASS);
     for (uint32_t base = gwarp * PASS; base < n; base += nwarps * PASS) {
         Raw pr[Q];
         uint32_t idx[Q];
@@ -275,13 +326,12 @@ __global__ void __launch_bounds__(256, 4) k_insert_win(__grid_constant__ const O
         uint32_t my_init = 0;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            uint32_t const i = base + q * TILES + tile;
-            bool const in = i < n && (!stencil || stencil[i]);
-            pr[q] = in ? Io<S>::load_pair(pairs, i) : Raw{};
+            pr[q] = nxt[q];
             uint64_t const key = S::key(pr[q]);
-            state[q] = !in ? kWinIdle : (key == a.empty_key ? kWinSettled : kWinOpen);
+            state[q] = !nin[q] ? kWinIdle : (key == a.empty_key ? kWinSettled : kWinOpen);
             if (int(r) == q && state[q] == kWinOpen) my_init = probe_init<S::key_bytes, B>(a.probe, key);
         }
+        load_pass(base + nwarps * PASS);
         Raw w[Q][ROUNDS];
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
@@ -292,20 +342,32 @@ __global__ void __launch_bounds__(256, 4) k_insert_win(__grid_constant__ const O
                     if (int(r) + t * G < B) w[q][t] = ld_win(slots + idx[q] + r + t * G);
             }
         }
+        {
+            Raw* wb[Q];
+            uint64_t key[Q], val[Q], found[Q];
+            int verdict[Q], slot[Q];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            uint32_t const i = base + q * TILES + tile;
-            uint64_t const key = S::key(pr[q]);
-            if (state[q] == kWinSettled) {  // the empty key itself: FAILED
-                if (r == 0) record(i, kFailed, 0, key, 0);
-                state[q] = kWinIdle;
+            for (int q = 0; q < Q; ++q) {
+                uint32_t const i = base + q * TILES + tile;
+                key[q] = S::key(pr[q]);
+                val[q] = S::value(pr[q]);
+                wb[q] = slots + idx[q];
+                verdict[q] = kFailed;
+                slot[q] = 0;
+                found[q] = 0;
+                if (state[q] == kWinSettled) {  // the empty key itself: FAILED
+                    if (r == 0) record(i, kFailed, 0, key[q], 0);
+                    state[q] = kWinIdle;
+                }
             }
-            int verdict = kFailed, slot = 0;
-            uint64_t found = 0;
-            tile_insert_window<S, B, G, ROUNDS, MODE>(a, slots + idx[q], w[q], key, S::value(pr[q]), r, tile_lane0,
-                                                      state[q], verdict, slot, found);
-            if (state[q] == kWinSettled && r == 0) record(i, verdict, idx[q] + slot, key, found);
-            enqueue(state[q] == kWinExhausted && r == 0, pr[q], idx[q], idx[q], i);
+            tile_insert_windows<S, B, G, Q, ROUNDS, MODE>(a, wb, w, key, val, r, tile_lane0, state, verdict, slot,
+                                                          found);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                uint32_t const i = base + q * TILES + tile;
+                if (state[q] == kWinSettled && r == 0) record(i, verdict[q], idx[q] + slot[q], key[q], found[q]);
+                enqueue(state[q] == kWinExhausted && r == 0, pr[q], idx[q], idx[q], i);
+            }
         }
         while (count >= PASS) follow();
     }

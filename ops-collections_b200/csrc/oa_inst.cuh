@@ -123,6 +123,10 @@ struct OaImpl {
     {
         return with_b(b, [&](auto bc) {
             constexpr int B = decltype(bc)::value;
+            // `newbits` holds two bitmaps of the table's slots: claimed in this
+            // batch, then lowered (a smaller input index than the claimer's)
+            uint32_t* lowered = newbits + (uint64_t(a.probe.capacity) + 31) / 32;
+            uint32_t const claim_bit = a.probe.capacity < kClaimBit ? kClaimBit : 0u;  // slot indices below 2^31 - 1
             bool placed = false;
             if constexpr (B > 1) {
                 if (!per_key_writes(a, B)) {
@@ -130,19 +134,22 @@ struct OaImpl {
                     o.pos = pos;
                     o.newbits = newbits;
                     o.owner = owner;
+                    o.claim_bit = claim_bit;
                     if (int st = launch_write<B, kInsIafPlace>(a, pairs, nullptr, n, o, s)) return st;
                     placed = true;
                 }
             }
             if (!placed) {
                 auto k1 = k_iaf_place<S, B>;
-                k1<<<grid_for((void const*)k1, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, n, pos, newbits, owner);
+                k1<<<grid_for((void const*)k1, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, n, pos, newbits, owner,
+                                                                                    claim_bit);
             }
             auto k2 = k_iaf_min<S>;
-            k2<<<grid_for((void const*)k2, kBlock, n, kBlock), kBlock, 0, s>>>(pos, newbits, owner, n);
+            k2<<<grid_for((void const*)k2, kBlock, n, kBlock), kBlock, 0, s>>>(pos, newbits, lowered, owner, n,
+                                                                                claim_bit);
             auto k3 = k_iaf_final<S>;
-            k3<<<grid_for((void const*)k3, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, pos, newbits, owner, found,
-                                                                                inserted, n);
+            k3<<<grid_for((void const*)k3, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, pos, newbits, lowered, owner,
+                                                                                found, inserted, n, claim_bit);
             return check_launch("insert_and_find (first wins) kernels");
         });
     }

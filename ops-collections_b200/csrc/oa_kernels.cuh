@@ -293,16 +293,25 @@ __global__ void __launch_bounds__(256) k_iaf_race(__grid_constant__ const OaArgs
 // sequentially in input order (the golden of tests/common/golden.h:104-131).
 //   place : every key finds or claims its slot; pos[i] = slot; a claiming
 //           thread marks the slot new and records itself as its owner;
-//   min   : inputs that landed on a new slot lower the owner to the least
-//           input index (atomicMin);
+//   min   : the other inputs on a new slot lower the owner to the least
+//           input index (atomicMin) and, when they did lower it, set the
+//           slot's bit in `lowered`;
 //   final : owner i is the inserted one; every other input on a new slot
 //           finds the owner's payload (read from the input, never a racing
 //           slot); inputs on old slots find the stored payload.
+// When the table has at most 2^31 slots, pos[i] of the input that claimed the
+// slot carries kClaimBit: min skips the claimers, and in final a claimer whose
+// slot was not lowered is the inserted one without reading owner[] and
+// without rewriting a slot its CAS already filled -- the common case costs
+// no random DRAM access after placement.  `lowered` is the bitmap right after
+// `newbits` (both cleared before place).
 // ----------------------------------------------------------------------------
+
+constexpr uint32_t kClaimBit = 0x80000000u;
 
 template <class S, int B>
 __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArgs a, void const* pairs, uint32_t n, uint32_t* pos,
-                                                   uint32_t* newbits, uint32_t* owner)
+                                                   uint32_t* newbits, uint32_t* owner, uint32_t claim_bit)
 {
     using Raw = typename S::Raw;
     Raw* slots = reinterpret_cast<Raw*>(a.slots);
@@ -332,6 +341,7 @@ __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArg
                             where = idx + j;
                             atomicOr(newbits + (where >> 5), 1u << (where & 31));
                             owner[where] = i;
+                            where |= claim_bit;
                             done = true;
                         } else if (S::key_eq(S::key(old), key)) {
                             where = idx + j;
@@ -352,34 +362,44 @@ __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArg
 __device__ __forceinline__ bool bit_set(uint32_t const* bits, uint32_t s) { return (bits[s >> 5] >> (s & 31)) & 1u; }
 
 template <class S>  // one copy per slot layout's translation unit
-__global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t const* newbits, uint32_t* owner,
-                                                 uint32_t n)
+__global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t const* newbits, uint32_t* lowered,
+                                                 uint32_t* owner, uint32_t n, uint32_t claim_bit)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t s = pos[i];
-        if (s != kNoSlot && bit_set(newbits, s) && owner[s] != i) atomicMin(owner + s, i);
+        uint32_t const p = pos[i];
+        if (p == kNoSlot || (p & claim_bit)) continue;  // failed, or the claimer itself
+        uint32_t const s = p & ~claim_bit;
+        if (!bit_set(newbits, s)) continue;
+        uint32_t const was = atomicMin(owner + s, i);
+        if (i < was) atomicOr(lowered + (s >> 5), 1u << (s & 31));
     }
 }
 
 template <class S>
 __global__ void __launch_bounds__(256) k_iaf_final(__grid_constant__ const OaArgs a, void const* pairs, uint32_t const* pos,
-                                                   uint32_t const* newbits, uint32_t const* owner, void* out_found,
-                                                   uint8_t* out_inserted, uint32_t n)
+                                                   uint32_t const* newbits, uint32_t const* lowered,
+                                                   uint32_t const* owner, void* out_found, uint8_t* out_inserted,
+                                                   uint32_t n, uint32_t claim_bit)
 {
     using Raw = typename S::Raw;
     Raw* slots = reinterpret_cast<Raw*>(a.slots);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t s = pos[i];
+        uint32_t const p = pos[i];
         uint64_t found = empty_payload<S>(a);
         uint8_t inserted = 0;
-        if (s != kNoSlot) {
-            if (bit_set(newbits, s)) {
+        if (p != kNoSlot) {
+            bool const claimed = (p & claim_bit) != 0;
+            uint32_t const s = p & ~claim_bit;
+            if (claimed && !bit_set(lowered, s)) {  // the claimer is the least index: its CAS stored its pair
+                inserted = 1;
+                found = S::value(Io<S>::load_pair(pairs, i));
+            } else if (bit_set(newbits, s)) {
                 uint32_t m = owner[s];
                 Raw pm = Io<S>::load_pair(pairs, m);
                 found = S::value(pm);
                 if (m == i) {
                     inserted = 1;
-                    assign_payload<S>(slots + s, S::key(pm), found);
+                    if (!claimed) assign_payload<S>(slots + s, S::key(pm), found);
                 }
             } else {
                 found = S::value(ld_rw(slots + s));

@@ -12,9 +12,12 @@ from helpers import dev
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("mode", ["atomic", "bulk"])
 @pytest.mark.parametrize("kdt", [np.uint32, np.int32, np.uint64, np.int64, np.float32])
 @pytest.mark.parametrize("num_blocks", [1, 7, 4096, 1 << 16])
-def test_bloom_add_contains_bit_exact(kdt, num_blocks):
+def test_bloom_add_contains_bit_exact(kdt, num_blocks, mode):
+    """Both Add paths of the default policy (64-bit atomics, TMA bulk ORs) set
+    exactly the oracle's bits."""
     import b2co
     import torch
     rng = np.random.default_rng(int(num_blocks) + np.dtype(kdt).itemsize)
@@ -27,6 +30,7 @@ def test_bloom_add_contains_bit_exact(kdt, num_blocks):
     ktorch = {np.uint32: torch.int32, np.int32: torch.int32, np.float32: torch.int32,
               np.uint64: torch.int64, np.int64: torch.int64}[kdt]
     f = b2co.BloomFilter(num_blocks, key_dtype=ktorch)
+    f.set_add_mode(b2co.BLOOM_ADD_BULK if mode == "bulk" else b2co.BLOOM_ADD_ATOMIC)
     kd = torch.from_numpy(keys.view(np.int32 if keys.itemsize == 4 else np.int64)).cuda()
     f.Add(kd[: n // 2])
     f.AddAsync(kd[n // 2:])
