@@ -591,6 +591,45 @@ def extra_measurements(t, keys, q50, out, stream, args):
     return res
 
 
+def fill_measurements(stream, reps=3):
+    """The headline table's fill on its own: StaticMap<int64,int64>, 2^28 slots
+    requested, first-wins InsertAndFind of the benchmark's insert streams to
+    load factor 0.5 and 0.8 (10% duplicate keys), `reps` times each into a
+    cleared table (clears not timed, scratch reserved beforehand, so no timed
+    region allocates); every run's inserted count is checked."""
+    import b2co
+    import torch
+    t = b2co.StaticMap(REQ_CAPACITY, -1, -1, key_dtype=torch.int64, value_dtype=torch.int64, bucket_size=5,
+                       probing=b2co.PROBE_DOUBLE, hash_kind=b2co.HASH_XXH32)
+    cap = t.Capacity()
+    t.ReserveInsertAndFind(sum(workload_sizes(cap, 0.8)))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    res = {}
+    for lf in (0.5, 0.8):
+        unique, dups = workload_sizes(cap, lf)
+        _, stream_keys, vals = make_insert_stream(unique, dups, "torch")
+        pairs = b2co.pack_pairs(stream_keys, vals)
+        del vals
+        found = torch.empty(stream_keys.numel(), dtype=torch.int64, device="cuda")
+        ins = torch.empty(stream_keys.numel(), dtype=torch.uint8, device="cuda")
+        runs = []
+        for _ in range(reps):
+            t.ClearAsync(stream=stream)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            t.InsertAndFindAsync(pairs, found, ins, stream=stream, mode=b2co.IAF_FIRST_WINS)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            assert int(ins.sum().item()) == unique
+            runs.append(e0.elapsed_time(e1))
+        key = f"lf{int(lf * 10):02d}"
+        res[f"fill_{key}_ms"] = [round(x, 3) for x in runs]
+        res[f"fill_{key}_gkeys"] = round(stream_keys.numel() / min(runs) / 1e6, 3)
+        res[f"fill_{key}_spread"] = round(max(runs) / min(runs) - 1.0, 4)
+        del pairs, found, ins, stream_keys
+    return res
+
+
 INSERT_SHAPES = [(1, 1), (2, 1), (2, 2), (4, 1), (4, 2), (4, 4), (8, 2), (8, 4)]
 
 
@@ -874,6 +913,17 @@ def batched_measurements(stream):
     out2 = torch.empty_like(out)
     ms = timed(lambda: per.FindPerTable(q, q_off.astype(np.uint64), out2), reps=2)
     res["batched_per_table_find_gkeys"] = round(2 * total / ms / 1e6, 3)
+    # the 4,096 per-table launches captured once in a CUDA graph and replayed:
+    # what a graph buys when the work is many small launches
+    graph = torch.cuda.CUDAGraph()
+    out2.zero_()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        per.FindPerTable(q, q_off.astype(np.uint64), out2)
+    ms = timed(lambda: graph.replay(), reps=2)
+    res["batched_per_table_graph_find_gkeys"] = round(2 * total / ms / 1e6, 3)
+    res["batched_per_table_graph_equals_group"] = bool(torch.equal(out2, ref))
+    del graph
     res["batched_per_table_equals_group"] = bool(torch.equal(out2, ref))
     res["batched_hits_found"] = bool(((ref != -1) == hit).all().item())
     return res
@@ -1228,7 +1278,7 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                 "launches": launches, "requests_per_launch": round(count / max(1, launches), 2),
                 "host_us_per_launch": round((s1["total_launch_host_ns"] - s0["total_launch_host_ns"])
                                             / max(1, launches) / 1e3, 1),
-                "copies": s1["copies"] - s0["copies"]}
+                "copies": s1["copies"] - s0["copies"], "packed_launches": s1["packed_launches"] - s0["packed_launches"]}
 
     run_rate(rates[0], 128)  # warm-up: first launches of every table
     out, plain = [], []
@@ -1237,6 +1287,15 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
         log(f"[served] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s, "
             f"{r['requests_per_launch']} req/launch, {r['host_us_per_launch']} us host/launch")
         out.append(r)
+    # the same server with every request copied on its own (coalesced launches, unpacked copies)
+    srv.set_packing(False)
+    unpacked = []
+    for rate in rates:
+        r = run_rate(rate, max(200, int(rate * seconds)))
+        log(f"[served unpacked] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s")
+        unpacked.append({k: r[k] for k in ("offered_req_s", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
+                                           "copies", "launches")})
+    srv.set_packing(True)
     # the baseline on the same schedule: one plain launch per request, one
     # request per table at a time (copy in, Find / InsertOrAssign, copy out)
     srv.set_plain(True)
@@ -1255,7 +1314,7 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                        "request_pool": pool, "mean_request_keys": round(float(np.mean(ns)), 1),
                        "seconds_per_rate": seconds, "host_buffers": "pinned",
                        "staging_grows": st["staging_grows"], "max_loop_gap_us": round(st["max_loop_gap_ns"] / 1e3, 1),
-                       "sweep": out, "plain_per_table_sweep": plain,
+                       "sweep": out, "unpacked_sweep": unpacked, "plain_per_table_sweep": plain,
                        "server_over_plain_gkeys": [round(a["gkeys_s"] / b["gkeys_s"], 3) for a, b in zip(out, plain)]}}
 
 
@@ -1318,7 +1377,7 @@ def main():
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity hint in bytes (0 = leave default)")
     ap.add_argument("--only", default="",
                     choices=["", "served", "batched", "bloom_hll", "hll", "multi", "roaring", "small_map",
-                             "insert", "dmap"],
+                             "insert", "dmap", "fill"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
     ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
     args = ap.parse_args()
@@ -1331,7 +1390,7 @@ def main():
         fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,
               "hll": lambda s: bloom_hll_measurements(s, bloom=False, hll_log2=args.hll_log2),
               "multi": multi_measurements, "roaring": roaring_measurements,
-              "small_map": small_map_measurements, "dmap": dynamic_map_measurements,
+              "small_map": small_map_measurements, "dmap": dynamic_map_measurements, "fill": fill_measurements,
               "insert": lambda st: insert_measurements(st, capacity_log2=args.capacity_log2,
                                                        shapes=INSERT_SHAPES if args.sweep else None)}[args.only]
         print(json.dumps(fn(torch.cuda.current_stream())), flush=True)

@@ -248,7 +248,7 @@ int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_
  * depend on it).  lanes_per_key 1 runs one lane per key (the reference's scan
  * as written); 2, 4 or 8 lanes share each bucket window with keys_per_tile
  * (1, 2 or 4) keys in flight per lane group.  (0, 0) restores the default:
- * 4 lanes, 2 keys (one lane per key for bucket size 1).  Layouts with 2-byte
+ * 4 lanes, 1 key (one lane per key for bucket size 1).  Layouts with 2-byte
  * or floating-point keys run the default window shape for any request other
  * than one lane per key. */
 int b2co_oa_set_write_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_tile);
@@ -357,6 +357,15 @@ int b2co_server_register_table(b2co_server* server, b2co_oa_table* table);
  * for the previous one to finish; different tables still overlap).  Set it
  * while no request is queued. */
 int b2co_server_set_plain(b2co_server* server, int plain);
+/* Packed copies (on by default): the requests of a coalesced launch are packed
+ * by a small pool of host threads into a pinned arena of the launch slot, so
+ * the launch issues one host-to-device and one device-to-host copy instead of
+ * one per request each way; results are scattered back to each request's
+ * buffer before it completes.  The copy engines' rate of operations, not
+ * their bandwidth, is what caps a server of many mid-sized requests.  The
+ * arenas (24 bytes per key of a launch of up to 4 Mi keys, per slot) are
+ * allocated with the server; larger launches copy per request. */
+int b2co_server_set_packing(b2co_server* server, int on);
 /* host_in: keys (Find/Contains) or pairs (Insert/InsertOrAssign); host_out:
  * payloads (Find) or 1-byte flags (Contains), unused otherwise. */
 int b2co_server_submit(b2co_server* server, b2co_oa_table* table, int op, const void* host_in, void* host_out,
@@ -392,6 +401,7 @@ typedef struct {
     uint64_t max_loop_gap_ns;       /* longest interval between two dispatcher polls */
     uint64_t total_launch_host_ns;  /* host time issuing all launches */
     uint64_t copies;                /* host<->device copies issued */
+    uint64_t packed_launches;       /* coalesced launches whose requests shared one copy each way */
 } b2co_server_stats_ex;
 int b2co_server_get_stats_ex(b2co_server* server, b2co_server_stats_ex* stats);
 /* Finishes every submitted request, then stops the dispatcher. */

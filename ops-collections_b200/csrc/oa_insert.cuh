@@ -188,8 +188,15 @@ __device__ __forceinline__ void tile_insert_windows(OaArgs const& a, typename S:
         if (state[q] == kWinOpen) state[q] = kWinExhausted;
 }
 
+// Resident blocks per SM the write kernel is compiled for: one key per lane
+// group fits 64 registers; more keys in flight keep their windows, snapshots
+// and CAS operands live at once and get the registers of two blocks per SM
+// instead of spilling.
+template <int Q>
+constexpr int kWriteMinBlocks = Q == 1 ? 4 : 2;
+
 template <class S, int B, int G, int Q, int MODE>
-__global__ void __launch_bounds__(256, 4) k_insert_win(__grid_constant__ const OaArgs a, void const* pairs,
+__global__ void __launch_bounds__(256, kWriteMinBlocks<Q>) k_insert_win(__grid_constant__ const OaArgs a, void const* pairs,
                                                        uint8_t const* stencil, uint32_t n, InsOut o)
 {
     static_assert(Q <= G && G <= 8 && (G & (G - 1)) == 0, "tile shape");

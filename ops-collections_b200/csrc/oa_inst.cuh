@@ -55,15 +55,15 @@ struct OaImpl {
                             cudaStream_t s)
     {
         uint32_t lanes = a.write_shape >> 8, items = a.write_shape & 0xffu;
-        if (lanes == 0) lanes = 4, items = 2;
+        if (lanes == 0) lanes = 4, items = 1;  // default: 4 lanes per window, one key per lane group
         void (*k)(OaArgs, void const*, uint8_t const*, uint32_t, InsOut) = nullptr;
         if constexpr (kAllShapes && B == 5) {  // other shapes: the common bucket size only (build time)
             if (lanes == 2) k = items >= 2 ? k_insert_win<S, B, 2, 2, MODE> : k_insert_win<S, B, 2, 1, MODE>;
             else if (lanes == 8) k = items >= 4 ? k_insert_win<S, B, 8, 4, MODE> : k_insert_win<S, B, 8, 2, MODE>;
-            else if (items == 1) k = k_insert_win<S, B, 4, 1, MODE>;
+            else if (items == 2) k = k_insert_win<S, B, 4, 2, MODE>;
             else if (items >= 4) k = k_insert_win<S, B, 4, 4, MODE>;
         }
-        if (!k) lanes = 4, items = 2, k = k_insert_win<S, B, 4, 2, MODE>;
+        if (!k) lanes = 4, items = 1, k = k_insert_win<S, B, 4, 1, MODE>;
         uint64_t const per_block = (kBlock / 32) * (32 / lanes) * items;
         k<<<grid_for((void const*)k, kBlock, n, per_block), kBlock, 0, s>>>(a, pairs, stencil, n, o);
         return check_launch("insert kernel");

@@ -40,19 +40,24 @@ int sm_count()
 
 uint32_t grid_for(void const* kernel, uint32_t block, uint64_t work, uint64_t per_block)
 {
-    // resident blocks per SM of this kernel, cached per kernel
+    // resident blocks per SM of this kernel at this block size, cached
+    struct Occ {
+        void const* kernel;
+        uint32_t block;
+        int per_sm;
+    };
     static std::mutex mu;
-    static std::vector<std::pair<void const*, int>> occ;
+    static std::vector<Occ> occ;
     int per_sm = 0;
     {
         std::lock_guard<std::mutex> g(mu);
         for (auto& e : occ)
-            if (e.first == kernel) per_sm = e.second;
+            if (e.kernel == kernel && e.block == block) per_sm = e.per_sm;
         if (per_sm == 0) {
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, int(block), 0) != cudaSuccess ||
                 per_sm <= 0)
                 per_sm = 1;
-            occ.emplace_back(kernel, per_sm);
+            occ.push_back(Occ{kernel, block, per_sm});
         }
     }
     uint64_t want = per_block ? (work + per_block - 1) / per_block : 1;

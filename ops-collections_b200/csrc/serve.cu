@@ -31,6 +31,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -82,6 +83,92 @@ struct Slot {
     char* buf = nullptr;  // persistent staging: [inputs | outputs | 2 counters]
     uint64_t cap = 0;
     unsigned long long* h_counters = nullptr;  // pinned (failed, assigned) of an Insert / IOA launch
+    // packed copies: pinned host arenas a coalesced launch's inputs are packed
+    // into (one copy in) and its outputs come back to (one copy out)
+    char* hin = nullptr;
+    char* hout = nullptr;
+    uint64_t hin_cap = 0, hout_cap = 0;
+    bool packed = false;  // the launch in flight returns its outputs through hout
+};
+
+// Host copies spread over a small pool of threads (the caller takes part):
+// packing requests' inputs into a launch's pinned arena and scattering its
+// outputs back.  Jobs are cut into pieces of at most kPiece bytes.
+class CopyPool {
+   public:
+    static constexpr uint64_t kPiece = 1ull << 20;
+    struct Copy {
+        void* dst;
+        void const* src;
+        uint64_t bytes;
+    };
+
+    explicit CopyPool(unsigned threads)
+    {
+        for (unsigned i = 0; i < threads; ++i) workers_.emplace_back([this] { work(); });
+    }
+    ~CopyPool()
+    {
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+    size_t threads() const { return workers_.size(); }
+
+    // Runs every copy; returns when all are done.
+    void run(std::vector<Copy> const& copies)
+    {
+        pieces_.clear();
+        for (auto const& c : copies)
+            for (uint64_t off = 0; off < c.bytes; off += kPiece)
+                pieces_.push_back(Copy{static_cast<char*>(c.dst) + off, static_cast<char const*>(c.src) + off,
+                                       std::min(kPiece, c.bytes - off)});
+        if (pieces_.empty()) return;
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            next_.store(0);
+            left_.store(pieces_.size());
+            ++epoch_;
+        }
+        cv_.notify_all();
+        drain();
+        while (left_.load(std::memory_order_acquire) != 0) std::this_thread::yield();
+    }
+
+   private:
+    void drain()
+    {
+        for (;;) {
+            size_t const i = next_.fetch_add(1);
+            if (i >= pieces_.size()) return;
+            std::memcpy(pieces_[i].dst, pieces_[i].src, pieces_[i].bytes);
+            left_.fetch_sub(1, std::memory_order_release);
+        }
+    }
+    void work()
+    {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> l(mu_);
+                cv_.wait(l, [&] { return stop_ || epoch_ != seen; });
+                if (stop_) return;
+                seen = epoch_;
+            }
+            drain();
+        }
+    }
+
+    std::vector<std::thread> workers_;
+    std::vector<Copy> pieces_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::atomic<size_t> next_{0}, left_{0};
+    uint64_t epoch_ = 0;
+    bool stop_ = false;
 };
 
 enum class Fit { kOk, kWait, kNever, kError };
@@ -95,6 +182,11 @@ struct b2co_server {
     // launch in flight (copy in, kernel, copy out, then the table's next
     // request); the baseline the coalescing server is measured against
     std::atomic<bool> plain{false};
+    // packed copies of coalesced launches: the pool and the slots' pinned
+    // arenas exist from creation; `pack` switches their use on and off
+    std::unique_ptr<CopyPool> packer;
+    std::atomic<bool> pack{true};
+    std::atomic<uint64_t> packed_launches{0};
 
     // submission side (in_mu)
     std::mutex in_mu;
@@ -155,6 +247,8 @@ struct b2co_server {
             }
             if (sl.done) cudaEventDestroy(sl.done);
             if (sl.h_counters) cudaFreeHost(sl.h_counters);
+            if (sl.hin) cudaFreeHost(sl.hin);
+            if (sl.hout) cudaFreeHost(sl.hout);
             sl = Slot{};
         }
         if (pool) cudaMemPoolDestroy(pool);
@@ -214,11 +308,27 @@ struct b2co_server {
         char* din = sl.buf;
         char* dout = sl.buf + align(in_total);
         auto* dcnt = reinterpret_cast<unsigned long long*>(dout + align(out_total));
+        // a coalesced launch packs its requests into the slot's pinned arena:
+        // one copy in and one copy out instead of one per request each way
+        sl.packed = packer && pack.load(std::memory_order_relaxed) && g.size() > 1 && in_total <= sl.hin_cap &&
+                    out_total <= sl.hout_cap;
         uint64_t off = 0;
-        for (auto* r : g) {
-            B2CO_CUDA(cudaMemcpyAsync(din + off, r->host_in, r->in_bytes, cudaMemcpyHostToDevice, s));
-            off += r->in_bytes;
+        if (sl.packed) {
+            std::vector<CopyPool::Copy> pack;
+            for (auto* r : g) {
+                pack.push_back(CopyPool::Copy{sl.hin + off, r->host_in, r->in_bytes});
+                off += r->in_bytes;
+            }
+            packer->run(pack);
+            B2CO_CUDA(cudaMemcpyAsync(din, sl.hin, in_total, cudaMemcpyHostToDevice, s));
             ++copies;
+            ++packed_launches;
+        } else {
+            for (auto* r : g) {
+                B2CO_CUDA(cudaMemcpyAsync(din + off, r->host_in, r->in_bytes, cudaMemcpyHostToDevice, s));
+                off += r->in_bytes;
+                ++copies;
+            }
         }
         int const op = h->info.op;
         bool const writes = is_write(h);
@@ -242,13 +352,20 @@ struct b2co_server {
             }
         }
         if (st) return st;
-        off = 0;
-        for (auto* r : g) {
-            if (r->out_bytes) {
-                B2CO_CUDA(cudaMemcpyAsync(r->host_out, dout + off, r->out_bytes, cudaMemcpyDeviceToHost, s));
+        if (sl.packed) {
+            if (out_total) {
+                B2CO_CUDA(cudaMemcpyAsync(sl.hout, dout, out_total, cudaMemcpyDeviceToHost, s));
                 ++copies;
             }
-            off += r->out_bytes;
+        } else {
+            off = 0;
+            for (auto* r : g) {
+                if (r->out_bytes) {
+                    B2CO_CUDA(cudaMemcpyAsync(r->host_out, dout + off, r->out_bytes, cudaMemcpyDeviceToHost, s));
+                    ++copies;
+                }
+                off += r->out_bytes;
+            }
         }
         B2CO_CUDA(cudaEventRecord(sl.done, s));
         sl.busy = true;
@@ -399,6 +516,15 @@ struct b2co_server {
                     r->info.failed = sl.h_counters[0];
                     r->info.assigned = sl.h_counters[1];
                 }
+            if (q == cudaSuccess && sl.packed) {  // the outputs came back packed: hand each request its part
+                std::vector<CopyPool::Copy> scatter;
+                uint64_t off = 0;
+                for (auto* r : sl.reqs) {
+                    if (r->out_bytes) scatter.push_back(CopyPool::Copy{r->host_out, sl.hout + off, r->out_bytes});
+                    off += r->out_bytes;
+                }
+                packer->run(scatter);
+            }
             sl.busy = false;
             std::vector<Request*> g;
             g.swap(sl.reqs);
@@ -565,6 +691,19 @@ int b2co_server_create(uint32_t max_inflight, uint64_t hbm_budget_bytes, uint64_
                 if (s->reserve(sl, per_slot, true) != Fit::kOk)
                     return fail(B2CO_ENOMEM, "staging reservation failed");
         for (auto& sl : s->slots) B2CO_CUDA(cudaStreamSynchronize(sl.stream));
+        // packed copies: a pinned arena per slot for a coalesced launch of up
+        // to 4 Mi keys (16-byte pairs in, 8-byte payloads out) and a pool of
+        // host threads that pack and scatter
+        uint64_t const keys = std::min<uint64_t>(s->max_batch_keys, 1ull << 22);
+        for (auto& sl : s->slots) {
+            B2CO_CUDA(cudaMallocHost(reinterpret_cast<void**>(&sl.hin), keys * 16));
+            B2CO_CUDA(cudaMallocHost(reinterpret_cast<void**>(&sl.hout), keys * 8));
+            sl.hin_cap = keys * 16;
+            sl.hout_cap = keys * 8;
+        }
+        unsigned const hw = std::max(2u, std::thread::hardware_concurrency());
+        s->packer.reset(new (std::nothrow) CopyPool(std::min(8u, hw / 2) - 1));
+        if (!s->packer) return fail(B2CO_ENOMEM, "host allocation failed");
         return B2CO_OK;
     };
     if (int st = setup()) {
@@ -573,6 +712,13 @@ int b2co_server_create(uint32_t max_inflight, uint64_t hbm_budget_bytes, uint64_
     }
     s->worker = std::thread([s] { s->run(); });
     *out = guard.release();
+    return B2CO_OK;
+}
+
+int b2co_server_set_packing(b2co_server* s, int on)
+{
+    if (!s) return fail(B2CO_EINVAL, "null server");
+    s->pack.store(on != 0);
     return B2CO_OK;
 }
 
@@ -647,6 +793,7 @@ int b2co_server_get_stats_ex(b2co_server* s, b2co_server_stats_ex* out)
     out->max_loop_gap_ns = s->max_gap_ns.load();
     out->total_launch_host_ns = s->launch_ns.load();
     out->copies = s->copies.load();
+    out->packed_launches = s->packed_launches.load();
     return B2CO_OK;
 }
 

@@ -96,10 +96,12 @@ def make_tables(contents):
     return tables
 
 
-def run(contents, reqs, max_inflight, sequential, max_batch_keys=0):
+def run(contents, reqs, max_inflight, sequential, max_batch_keys=0, packing=True, plain=False):
     import b2co
     tables = make_tables(contents)
     srv = b2co.Server(max_inflight=max_inflight, hbm_budget_bytes=8 << 30, max_batch_keys=max_batch_keys)
+    srv.set_packing(packing)
+    srv.set_plain(plain)
     for m in tables:
         srv.register(m)
     ins, bufs, infos, ids = [], [], [], []
@@ -153,6 +155,33 @@ def test_results_same_alone_and_in_the_mix():
     assert b_stats["requests_launched"] == len(reqs)
     # staging was sized at creation: no buffer grew under traffic
     assert b_stats["staging_grows"] == 8
+    # coalesced launches shared one copy each way (packed), fewer copies than requests
+    assert b_stats["packed_launches"] > 0
+    assert b_stats["copies"] < a_stats["copies"]
+
+
+def test_mix_unpacked_and_plain_modes_give_the_same_results():
+    """The coalescing server with per-request copies, and the plain baseline
+    (one launch per request, one request per table at a time), give the
+    sequential results too."""
+    import b2co
+    contents = initial_contents()
+    reqs = make_requests(contents)
+    e_out = None
+    for kw in ({"packing": False}, {"plain": True}):
+        out, info, pairs, stats, cap = run(contents, reqs, 8, sequential=False, **kw)
+        if e_out is None:
+            e_out, e_counts, e_pairs = expected(contents, reqs, cap)
+        for i, (t, op, data) in enumerate(reqs):
+            if op == b2co.OP_FIND:
+                assert np.array_equal(out[i], e_out[i]), (kw, i)
+            else:
+                assert (info[i].failed, info[i].assigned) == e_counts[i], (kw, i)
+        for x, e in zip(pairs, e_pairs):
+            assert np.array_equal(x, e), kw
+        assert stats["packed_launches"] == 0, kw
+        if kw.get("plain"):
+            assert stats["launches"] == len(reqs)
 
 
 def test_scheduled_arrivals_and_small_batches():
