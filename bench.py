@@ -1009,18 +1009,17 @@ def bloom_part(f_time, g, peak):
     ms = time_once(lambda: f.AddAsync(adds))
     res["bloom_add_gkeys"] = round(n / ms / 1e6, 3)
     res["bloom_add_hbm_frac"] = round(n * 72 / (ms / 1e3) / 1e9 / peak, 4)
-    # the same Add through TMA bulk reductions (one 32-byte OR per key); same bits
-    atomic_words = f.words()
-    f.set_add_mode(b2co.BLOOM_ADD_BULK)
+    # the same Add through 64-bit atomics (the alternative path); same bits
+    bulk_words = f.words()
+    f.set_add_mode(b2co.BLOOM_ADD_ATOMIC)
     f.Clear()
     f.AddAsync(adds)
     f.Clear()
     ms = time_once(lambda: f.AddAsync(adds))
-    res["bloom_add_bulk_gkeys"] = round(n / ms / 1e6, 3)
-    res["bloom_add_bulk_hbm_frac"] = round(n * 72 / (ms / 1e3) / 1e9 / peak, 4)
-    res["bloom_add_bulk_equals_atomic"] = bool(np.array_equal(f.words(), atomic_words))
-    del atomic_words
-    f.set_add_mode(b2co.BLOOM_ADD_ATOMIC)
+    res["bloom_add_atomic_gkeys"] = round(n / ms / 1e6, 3)
+    res["bloom_add_atomic_equals_bulk"] = bool(np.array_equal(f.words(), bulk_words))
+    del bulk_words
+    f.set_add_mode(b2co.BLOOM_ADD_BULK)
     out = torch.empty(q.numel(), dtype=torch.uint8, device="cuda")
     f.ContainsAsync(q, out)
     ms = time_once(lambda: f.ContainsAsync(q, out))
@@ -1287,15 +1286,15 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
         log(f"[served] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s, "
             f"{r['requests_per_launch']} req/launch, {r['host_us_per_launch']} us host/launch")
         out.append(r)
-    # the same server with every request copied on its own (coalesced launches, unpacked copies)
-    srv.set_packing(False)
-    unpacked = []
+    # the same server with coalesced launches packed into one copy each way (host threads pack and scatter)
+    srv.set_packing(True)
+    packed = []
     for rate in rates:
         r = run_rate(rate, max(200, int(rate * seconds)))
-        log(f"[served unpacked] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s")
-        unpacked.append({k: r[k] for k in ("offered_req_s", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
-                                           "copies", "launches")})
-    srv.set_packing(True)
+        log(f"[served packed] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s")
+        packed.append({k: r[k] for k in ("offered_req_s", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
+                                         "copies", "launches", "packed_launches")})
+    srv.set_packing(False)
     # the baseline on the same schedule: one plain launch per request, one
     # request per table at a time (copy in, Find / InsertOrAssign, copy out)
     srv.set_plain(True)
@@ -1314,7 +1313,7 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                        "request_pool": pool, "mean_request_keys": round(float(np.mean(ns)), 1),
                        "seconds_per_rate": seconds, "host_buffers": "pinned",
                        "staging_grows": st["staging_grows"], "max_loop_gap_us": round(st["max_loop_gap_ns"] / 1e3, 1),
-                       "sweep": out, "unpacked_sweep": unpacked, "plain_per_table_sweep": plain,
+                       "sweep": out, "packed_sweep": packed, "plain_per_table_sweep": plain,
                        "server_over_plain_gkeys": [round(a["gkeys_s"] / b["gkeys_s"], 3) for a, b in zip(out, plain)]}}
 
 

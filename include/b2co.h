@@ -357,13 +357,14 @@ int b2co_server_register_table(b2co_server* server, b2co_oa_table* table);
  * for the previous one to finish; different tables still overlap).  Set it
  * while no request is queued. */
 int b2co_server_set_plain(b2co_server* server, int plain);
-/* Packed copies (on by default): the requests of a coalesced launch are packed
+/* Packed copies (off by default): the requests of a coalesced launch are packed
  * by a small pool of host threads into a pinned arena of the launch slot, so
  * the launch issues one host-to-device and one device-to-host copy instead of
  * one per request each way; results are scattered back to each request's
  * buffer before it completes.  The copy engines' rate of operations, not
- * their bandwidth, is what caps a server of many mid-sized requests.  The
- * arenas (24 bytes per key of a launch of up to 4 Mi keys, per slot) are
+ * their bandwidth, limits a server of many small requests; with mid-sized
+ * requests the host copies cost more than the copy operations they save.
+ * The arenas (24 bytes per key of a launch of up to 4 Mi keys, per slot) are
  * allocated with the server; larger launches copy per request. */
 int b2co_server_set_packing(b2co_server* server, int on);
 /* host_in: keys (Find/Contains) or pairs (Insert/InsertOrAssign); host_out:
@@ -545,7 +546,7 @@ int b2co_bloom_add(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream
  * four 64-bit atomic ORs per key from the SM.  B2CO_BLOOM_ADD_BULK: one
  * 32-byte TMA bulk reduction (OR) per key from shared memory.  No reference
  * counterpart (the reference chooses between atomics and a routed path by
- * batch size, bloom_filter_launch.inl:131-240). */
+ * batch size, bloom_filter_launch.inl:131-240).  The default is BULK. */
 typedef enum { B2CO_BLOOM_ADD_ATOMIC = 0, B2CO_BLOOM_ADD_BULK = 1 } b2co_bloom_add_mode;
 int b2co_bloom_set_add_mode(b2co_bloom* filter, int mode);
 int b2co_bloom_add_async(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream stream);

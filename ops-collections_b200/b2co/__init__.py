@@ -546,7 +546,7 @@ class Server:
         _call("b2co_server_register_table", self._h, table._h)
 
     def set_packing(self, on: bool):
-        """Packed copies of coalesced launches (on by default)."""
+        """Packed copies of coalesced launches (off by default)."""
         _call("b2co_server_set_packing", self._h, C.c_int(1 if on else 0))
 
     def set_plain(self, plain: bool):
@@ -924,7 +924,7 @@ class BloomFilter:
         return p.value
 
     def set_add_mode(self, mode: int):
-        """BLOOM_ADD_ATOMIC (64-bit atomics) or BLOOM_ADD_BULK (TMA bulk OR) for the default policy's Add."""
+        """BLOOM_ADD_BULK (TMA bulk OR, the default) or BLOOM_ADD_ATOMIC (64-bit atomics) for the default policy's Add."""
         _call("b2co_bloom_set_add_mode", self._h, C.c_int(mode))
 
     def words(self) -> np.ndarray:

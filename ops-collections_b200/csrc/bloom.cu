@@ -4,10 +4,11 @@
 // of word w at (salt[w * bitsPerWord + b] * lower hash) >> 27.
 //
 // B200 design for the default policy (W = 8, one bit per word): a block is
-// exactly one 32-byte L2 sector.  Add issues the block's 8 word bits as four
-// 64-bit atomic ORs that need no return value (RED), all to that one sector;
-// lanes of a warp that hit the same block are merged first (match_any) so each
-// distinct block takes one set of REDs.  Contains reads the sector with two
+// exactly one 32-byte L2 sector.  Add stages the block's 8 word bits in shared
+// memory and ORs the whole sector into the filter with one TMA bulk reduction
+// (cp.reduce.async.bulk .or.b32); the alternative issues them as four 64-bit
+// atomic ORs that need no return value (RED), all to that one sector, with
+// lanes of a warp that hit the same block merged first (match_any).  Contains reads the sector with two
 // 16-byte loads.  Other policies run one key per thread: W/2 64-bit REDs (one
 // 32-bit RED for W = 1) and vector loads of the block.  Merge/Intersect stream
 // 16 bytes per lane (4 when the word count is not a multiple of 4).
@@ -243,7 +244,7 @@ cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 
 struct b2co_bloom {
     uint32_t* words = nullptr;
-    int add_mode = B2CO_BLOOM_ADD_ATOMIC;  // default-policy Add: 64-bit atomics or bulk reductions
+    int add_mode = B2CO_BLOOM_ADD_BULK;  // default-policy Add: bulk reductions (measured faster) or 64-bit atomics
     uint64_t num_blocks = 0;
     uint32_t key_bytes = 0;
     uint64_t seed = 0;

@@ -185,7 +185,7 @@ struct b2co_server {
     // packed copies of coalesced launches: the pool and the slots' pinned
     // arenas exist from creation; `pack` switches their use on and off
     std::unique_ptr<CopyPool> packer;
-    std::atomic<bool> pack{true};
+    std::atomic<bool> pack{false};
     std::atomic<uint64_t> packed_launches{0};
 
     // submission side (in_mu)
