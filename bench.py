@@ -307,8 +307,13 @@ def run_gpu(args):
     fill_ms = e0.elapsed_time(e1)
     n_inserted = int(inserted.sum().item())
     assert n_inserted == unique, (n_inserted, unique)
-    del found, inserted
+    # the fill's inputs and outputs, kept on the host for the full-size parity check after timing
+    fill_host = None
+    if rank == 0 and not args.no_host:
+        fill_host = (stream_keys.cpu().numpy(), vals.cpu().numpy(), found.cpu().numpy(), inserted.cpu().numpy())
+    del found, inserted, pairs
     log(f"[bench] capacity {cap}, unique {unique}, stream {stream_keys.numel()}, fill {fill_ms:.1f} ms")
+    del stream_keys, vals
 
     q = make_queries(keys, N_QUERIES, 0.5, "torch")
     out = torch.empty(N_QUERIES, dtype=torch.int64, device="cuda")
@@ -359,8 +364,9 @@ def run_gpu(args):
         extra["find_shape_sweep_gkeys"] = sweep
     windows_mean, cpu = None, None
     if rank == 0 and not args.no_host:
-        windows_mean, cpu, parity = host_side_checks(t, q, out, args)
-        extra["oracle_parity_sample"] = parity
+        windows_mean, cpu, parity = host_side_checks(t, q, out, args, fill_host)
+        extra["parity_full_size"] = parity
+        del fill_host
     bytes_per_query = 8 + 8 + 80 * (windows_mean if windows_mean else 1.0)
     achieved = N_QUERIES * bytes_per_query / (ms_per_step / 1e3) / 1e9
     traffic = profiled_traffic()
@@ -473,20 +479,39 @@ def window_gather_ceiling(t, stream, find_gkeys, windows_mean):
     return out
 
 
-def host_side_checks(t, q, out, args):
-    """Probe windows per query (exact, oracle over the device table's bytes),
-    an oracle parity sample and the CPU baseline on the host cores."""
+def host_side_checks(t, q, out, args, fill_host):
+    """Exact parity of the timed workload at full size, the probe windows per
+    query (exact, oracle over the device table's bytes) and the CPU baseline
+    on the host cores.  Parity: the oracle refills the table sequentially from
+    the same insert stream (the first-wins golden) and must give every found
+    value and inserted flag of the device fill and the same stored pair set;
+    the last timed Find's 2^27 outputs must equal the oracle's Find on its own
+    table.  All of it runs after the timed region."""
     import oracle
     import torch
+    threads = os.cpu_count() or 1
     t0 = time.perf_counter()
+    d = oracle.Table(np.int64, np.int64, t.Capacity(), 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, -1, -1)
+    d.load_slots(t.dump_slots())
     o = oracle.Table(np.int64, np.int64, t.Capacity(), 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, -1, -1)
-    o.load_slots(t.dump_slots())
-    log(f"[bench] table copied to host in {time.perf_counter() - t0:.1f} s")
+    s_keys, s_vals, dev_found, dev_ins = fill_host
+    exp_found, exp_ins = o.insert_and_find(s_keys, s_vals)
+    t1 = time.perf_counter()
+    same, n_o, n_d, mism = o.same_pairs(d, threads)
+    qh = q.cpu().numpy()
+    exp = o.find_parallel(qh, threads)
+    parity = {"fill_inputs": int(len(s_keys)),
+              "fill_found_and_flags_identical": bool(np.array_equal(exp_found, dev_found)
+                                                     and np.array_equal(exp_ins, dev_ins)),
+              "stored_pairs_identical": bool(same), "stored_pairs": int(n_d),
+              "find_queries": int(len(qh)), "find_identical": bool(np.array_equal(exp, out.cpu().numpy())),
+              "oracle_fill_s": round(t1 - t0, 1)}
+    log(f"[bench] full-size parity {parity} in {time.perf_counter() - t0:.1f} s")
+    del o, exp_found, exp_ins, exp
     sample = 1 << 22
-    qs = q[:sample].cpu().numpy()
-    exp, win = o.find(qs)
-    parity = {"queries": sample, "identical": bool(np.array_equal(exp, out[:sample].cpu().numpy()))}
+    _, win = d.find(qh[:sample])
     windows_mean = float(win.mean())
+    o = d
     cpu = None
     if not args.no_cpu:
         threads = os.cpu_count() or 1

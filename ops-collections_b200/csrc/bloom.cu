@@ -89,19 +89,26 @@ __global__ void __launch_bounds__(256) k_bloom_add(uint32_t* words, uint32_t nbl
 // cp.reduce.async.bulk .or.b32 (element-wise atomic in L2), instead of four
 // 64-bit atomics from the SM.  Each thread double-buffers its slot: before
 // reusing a slot it waits until the bulk operation that read it has read it.
+// Slots per thread: bulk reductions a thread may have in flight.
+#ifndef B2CO_BLOOM_BULK_DEPTH
+#define B2CO_BLOOM_BULK_DEPTH 2
+#endif
+
 template <int KB>
 __global__ void __launch_bounds__(256) k_bloom_add_bulk(uint32_t* words, uint32_t nblocks, uint64_t seed,
                                                         void const* keys, uint8_t const* stencil, uint64_t n)
 {
-    __shared__ alignas(128) uint32_t stage[2][256][8];
+    constexpr int D = B2CO_BLOOM_BULK_DEPTH;
+    static_assert(D >= 2 && D <= 8, "bulk depth");
+    __shared__ alignas(128) uint32_t stage[D][256][8];
     uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
     uint32_t b = 0;
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
         if (stencil && !stencil[i]) continue;
         uint32_t block, lower;
         locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower);
-        // the bulk operation issued two keys ago read this slot: wait for that read
-        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+        // the bulk operation issued D keys ago read this slot: wait for that read
+        asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(D - 1) : "memory");
         uint32_t* slot = stage[b][threadIdx.x];
 #pragma unroll
         for (int q = 0; q < 2; ++q)
@@ -113,7 +120,7 @@ __global__ void __launch_bounds__(256) k_bloom_add_bulk(uint32_t* words, uint32_
                      "r"(smem_u32(slot))
                      : "memory");
         asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-        b ^= 1u;
+        b = b + 1 == D ? 0 : b + 1;
     }
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // every reduction done before the slots go away
 }

@@ -192,8 +192,11 @@ __device__ __forceinline__ void tile_insert_windows(OaArgs const& a, typename S:
 // group fits 64 registers; more keys in flight keep their windows, snapshots
 // and CAS operands live at once and get the registers of two blocks per SM
 // instead of spilling.
+#ifndef B2CO_WRITE_MINB1
+#define B2CO_WRITE_MINB1 4
+#endif
 template <int Q>
-constexpr int kWriteMinBlocks = Q == 1 ? 4 : 2;
+constexpr int kWriteMinBlocks = Q == 1 ? B2CO_WRITE_MINB1 : 2;
 
 template <class S, int B, int G, int Q, int MODE>
 __global__ void __launch_bounds__(256, kWriteMinBlocks<Q>) k_insert_win(__grid_constant__ const OaArgs a, void const* pairs,
