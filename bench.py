@@ -840,6 +840,9 @@ def mix32_torch(x):
     return x ^ (x >> 16)
 
 
+BATCHED_TABLES = 4096
+
+
 def batched_workload():
     """The batched workload's inputs, on the device: 4,096 StaticMap<int32,int32>
     tables with log-normal key counts (median 32,768, sigma(log2) = 2.0, clipped
@@ -850,7 +853,7 @@ def batched_workload():
     import torch
     import b2co
     rng = np.random.default_rng(SEED + 11)
-    count = 4096
+    count = BATCHED_TABLES
     sizes = np.clip(np.round(np.exp2(rng.normal(15.0, 2.0, size=count))), 1024, 4194304).astype(np.int64)
     total = int(sizes.sum())
     ins_off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
@@ -1302,7 +1305,8 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                 "launches": launches, "requests_per_launch": round(count / max(1, launches), 2),
                 "host_us_per_launch": round((s1["total_launch_host_ns"] - s0["total_launch_host_ns"])
                                             / max(1, launches) / 1e3, 1),
-                "copies": s1["copies"] - s0["copies"], "packed_launches": s1["packed_launches"] - s0["packed_launches"]}
+                "copies": s1["copies"] - s0["copies"], "packed_launches": s1["packed_launches"] - s0["packed_launches"],
+                "direct_launches": s1["direct_launches"] - s0["direct_launches"]}
 
     run_rate(rates[0], 128)  # warm-up: first launches of every table
     out, plain = [], []
@@ -1311,14 +1315,17 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
         log(f"[served] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s, "
             f"{r['requests_per_launch']} req/launch, {r['host_us_per_launch']} us host/launch")
         out.append(r)
-    # the same server with coalesced launches packed into one copy each way (host threads pack and scatter)
-    srv.set_packing(True)
-    packed = []
-    for rate in rates:
-        r = run_rate(rate, max(200, int(rate * seconds)))
-        log(f"[served packed] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s")
-        packed.append({k: r[k] for k in ("offered_req_s", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
-                                         "copies", "launches", "packed_launches")})
+    # the same server with every result copied out per request, and with
+    # coalesced requests packed into one copy each way by host threads
+    srv.set_direct_results(False)
+    copied, packed = [], []
+    for arm, lst in (("copied", copied), ("packed", packed)):
+        srv.set_packing(arm == "packed")
+        for rate in rates:
+            r = run_rate(rate, max(200, int(rate * seconds)))
+            log(f"[served {arm}] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s")
+            lst.append({k: r[k] for k in ("offered_req_s", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
+                                          "copies", "launches", "packed_launches")})
     srv.set_packing(False)
     # the baseline on the same schedule: one plain launch per request, one
     # request per table at a time (copy in, Find / InsertOrAssign, copy out)
@@ -1329,6 +1336,7 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
         plain.append({k: r[k] for k in ("offered_req_s", "requests", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
                                         "launches")})
     srv.set_plain(False)
+    srv.set_direct_results(True)
     st = srv.stats()
     srv.close()
     del tables
@@ -1338,7 +1346,8 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                        "request_pool": pool, "mean_request_keys": round(float(np.mean(ns)), 1),
                        "seconds_per_rate": seconds, "host_buffers": "pinned",
                        "staging_grows": st["staging_grows"], "max_loop_gap_us": round(st["max_loop_gap_ns"] / 1e3, 1),
-                       "sweep": out, "packed_sweep": packed, "plain_per_table_sweep": plain,
+                       "sweep": out, "copied_results_sweep": copied, "packed_sweep": packed,
+                       "plain_per_table_sweep": plain,
                        "server_over_plain_gkeys": [round(a["gkeys_s"] / b["gkeys_s"], 3) for a, b in zip(out, plain)]}}
 
 
@@ -1404,11 +1413,13 @@ def main():
                              "insert", "dmap", "fill"],
                     help="run one secondary measurement alone and print its JSON (not the headline line)")
     ap.add_argument("--hll-log2", type=int, default=30, help="HyperLogLog adds 2^k with --only hll (profiling)")
+    ap.add_argument("--batched-tables", type=int, default=4096, help="tables of the batched workload (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("warmup must be >= 3")
-    global REQ_CAPACITY, N_QUERIES
+    global REQ_CAPACITY, N_QUERIES, BATCHED_TABLES
     REQ_CAPACITY, N_QUERIES = 1 << args.capacity_log2, 1 << args.queries_log2
+    BATCHED_TABLES = args.batched_tables
     if args.only:
         import torch
         fn = {"served": served_measurements, "batched": batched_measurements, "bloom_hll": bloom_hll_measurements,

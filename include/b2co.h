@@ -367,6 +367,13 @@ int b2co_server_set_plain(b2co_server* server, int plain);
  * The arenas (24 bytes per key of a launch of up to 4 Mi keys, per slot) are
  * allocated with the server; larger launches copy per request. */
 int b2co_server_set_packing(b2co_server* server, int on);
+/* Direct results (on by default): a lookup launch whose requests' result
+ * buffers are pinned host memory gets its results written into them by the
+ * GPU (one small kernel of SM stores over PCIe per launch) instead of one
+ * device-to-host copy per request, so a lookup costs the copy engines one
+ * operation, its keys in.  Requests with pageable result buffers are copied
+ * as before.  In plain mode the same applies per request. */
+int b2co_server_set_direct_results(b2co_server* server, int on);
 /* host_in: keys (Find/Contains) or pairs (Insert/InsertOrAssign); host_out:
  * payloads (Find) or 1-byte flags (Contains), unused otherwise. */
 int b2co_server_submit(b2co_server* server, b2co_oa_table* table, int op, const void* host_in, void* host_out,
@@ -403,6 +410,7 @@ typedef struct {
     uint64_t total_launch_host_ns;  /* host time issuing all launches */
     uint64_t copies;                /* host<->device copies issued */
     uint64_t packed_launches;       /* coalesced launches whose requests shared one copy each way */
+    uint64_t direct_launches;       /* lookup launches whose results the GPU wrote into the host buffers */
 } b2co_server_stats_ex;
 int b2co_server_get_stats_ex(b2co_server* server, b2co_server_stats_ex* stats);
 /* Finishes every submitted request, then stops the dispatcher. */

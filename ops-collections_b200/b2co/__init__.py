@@ -521,7 +521,7 @@ class Server:
 
     _STATS_EX = ("launches", "requests_launched", "bytes_in_use", "staging_bytes", "staging_grows",
                  "max_launch_host_ns", "max_reserve_host_ns", "max_loop_gap_ns", "total_launch_host_ns", "copies",
-                 "packed_launches")
+                 "packed_launches", "direct_launches")
 
     def __init__(self, max_inflight=8, hbm_budget_bytes=150 << 30, max_batch_keys=0):
         L = lib()
@@ -548,6 +548,10 @@ class Server:
     def set_packing(self, on: bool):
         """Packed copies of coalesced launches (off by default)."""
         _call("b2co_server_set_packing", self._h, C.c_int(1 if on else 0))
+
+    def set_direct_results(self, on: bool):
+        """Lookup results written by the GPU into pinned host buffers (on by default)."""
+        _call("b2co_server_set_direct_results", self._h, C.c_int(1 if on else 0))
 
     def set_plain(self, plain: bool):
         """Plain mode: one launch per request, one request per table at a time (the baseline)."""

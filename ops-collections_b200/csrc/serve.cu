@@ -63,12 +63,49 @@ struct Request {
     b2co_oa_table* table = nullptr;
     void const* host_in = nullptr;
     void* host_out = nullptr;
+    void* out_dev = nullptr;  // host_out as the GPU addresses it, when it is pinned (else nullptr)
     uint64_t in_bytes = 0, out_bytes = 0;
     bool taken = false;  // admitted (possibly ahead of the queue's head); popped lazily
     std::atomic<bool> done{false};
 };
 
 bool is_write(Request const* r) { return r->info.op == B2CO_OP_INSERT || r->info.op == B2CO_OP_INSERT_OR_ASSIGN; }
+
+// Direct results: a lookup launch's results go from the device staging straight
+// into the requests' pinned host buffers with SM stores over PCIe (one kernel
+// for up to kScatterMax requests) instead of one device-to-host copy per request.
+constexpr uint32_t kScatterMax = 32;
+struct ScatterEntry {
+    void* dst;
+    uint64_t off, bytes;
+};
+struct ScatterList {
+    uint32_t count;
+    ScatterEntry e[kScatterMax];
+};
+
+// Block row y copies entry y; 16-byte stores when both ends and the length
+// allow it, 8- or 1-byte stores otherwise.
+__global__ void __launch_bounds__(256) k_scatter_out(char const* src, __grid_constant__ const ScatterList L)
+{
+    for (uint32_t j = blockIdx.y; j < L.count; j += gridDim.y) {
+        ScatterEntry const e = L.e[j];
+        char const* from = src + e.off;
+        char* to = static_cast<char*>(e.dst);
+        uint64_t const step = uint64_t(gridDim.x) * blockDim.x;
+        uint64_t const t0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+        uintptr_t const al = reinterpret_cast<uintptr_t>(from) | reinterpret_cast<uintptr_t>(to) | e.bytes;
+        if ((al & 15) == 0) {
+            for (uint64_t i = t0; i < e.bytes / 16; i += step)
+                reinterpret_cast<uint4*>(to)[i] = reinterpret_cast<uint4 const*>(from)[i];
+        } else if ((al & 7) == 0) {
+            for (uint64_t i = t0; i < e.bytes / 8; i += step)
+                reinterpret_cast<unsigned long long*>(to)[i] = reinterpret_cast<unsigned long long const*>(from)[i];
+        } else {
+            for (uint64_t i = t0; i < e.bytes; i += step) to[i] = from[i];
+        }
+    }
+}
 
 // How far past the head the dispatcher looks for lookups to coalesce.
 constexpr size_t kCoalesceScan = 4096;
@@ -186,7 +223,8 @@ struct b2co_server {
     // arenas exist from creation; `pack` switches their use on and off
     std::unique_ptr<CopyPool> packer;
     std::atomic<bool> pack{false};
-    std::atomic<uint64_t> packed_launches{0};
+    std::atomic<bool> direct{true};  // lookups write results straight into pinned host buffers
+    std::atomic<uint64_t> packed_launches{0}, direct_launches{0};
 
     // submission side (in_mu)
     std::mutex in_mu;
@@ -308,10 +346,13 @@ struct b2co_server {
         char* din = sl.buf;
         char* dout = sl.buf + align(in_total);
         auto* dcnt = reinterpret_cast<unsigned long long*>(dout + align(out_total));
-        // a coalesced launch packs its requests into the slot's pinned arena:
-        // one copy in and one copy out instead of one per request each way
-        sl.packed = packer && pack.load(std::memory_order_relaxed) && g.size() > 1 && in_total <= sl.hin_cap &&
-                    out_total <= sl.hout_cap;
+        // lookups whose result buffers are pinned get their results written by
+        // the GPU (no copy out); else a coalesced launch may pack its requests
+        // into the slot's pinned arena (one copy in and one copy out)
+        bool direct_results = !is_write(h) && direct.load(std::memory_order_relaxed);
+        for (auto* r : g) direct_results = direct_results && r->out_dev;
+        sl.packed = !direct_results && packer && pack.load(std::memory_order_relaxed) && g.size() > 1 &&
+                    in_total <= sl.hin_cap && out_total <= sl.hout_cap;
         uint64_t off = 0;
         if (sl.packed) {
             std::vector<CopyPool::Copy> pack;
@@ -352,7 +393,25 @@ struct b2co_server {
             }
         }
         if (st) return st;
-        if (sl.packed) {
+        if (direct_results) {
+            ScatterList L{};
+            uint64_t o = 0;
+            size_t done = 0;
+            while (done < g.size()) {
+                L.count = 0;
+                uint64_t most = 0;
+                for (; done < g.size() && L.count < kScatterMax; ++done) {
+                    Request* r = g[done];
+                    L.e[L.count++] = ScatterEntry{r->out_dev, o, r->out_bytes};
+                    o += r->out_bytes;
+                    most = std::max(most, r->out_bytes);
+                }
+                uint32_t const gx = uint32_t(std::min<uint64_t>(64, (most + 4095) / 4096 + 1));
+                k_scatter_out<<<dim3(gx, L.count), 256, 0, s>>>(dout, L);
+                B2CO_CUDA(cudaGetLastError());
+            }
+            ++direct_launches;
+        } else if (sl.packed) {
             if (out_total) {
                 B2CO_CUDA(cudaMemcpyAsync(sl.hout, dout, out_total, cudaMemcpyDeviceToHost, s));
                 ++copies;
@@ -598,6 +657,14 @@ int make_request(b2co_request_desc const& d, std::unique_ptr<Request>& out)
     r.info.arrival_ns = d.arrival_ns;
     r.in_bytes = d.n * (lookup ? kb : sb);
     r.out_bytes = op == B2CO_OP_FIND ? d.n * pb : (op == B2CO_OP_CONTAINS ? d.n : 0);
+    if (lookup) {  // a pinned result buffer the GPU can address (checked here, on the submitting thread)
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, d.host_out) == cudaSuccess && pa.type == cudaMemoryTypeHost &&
+            pa.devicePointer)
+            r.out_dev = pa.devicePointer;
+        else
+            cudaGetLastError();
+    }
     return B2CO_OK;
 }
 
@@ -722,6 +789,13 @@ int b2co_server_set_packing(b2co_server* s, int on)
     return B2CO_OK;
 }
 
+int b2co_server_set_direct_results(b2co_server* s, int on)
+{
+    if (!s) return fail(B2CO_EINVAL, "null server");
+    s->direct.store(on != 0);
+    return B2CO_OK;
+}
+
 int b2co_server_set_plain(b2co_server* s, int plain)
 {
     if (!s) return fail(B2CO_EINVAL, "null server");
@@ -794,6 +868,7 @@ int b2co_server_get_stats_ex(b2co_server* s, b2co_server_stats_ex* out)
     out->total_launch_host_ns = s->launch_ns.load();
     out->copies = s->copies.load();
     out->packed_launches = s->packed_launches.load();
+    out->direct_launches = s->direct_launches.load();
     return B2CO_OK;
 }
 

@@ -96,12 +96,13 @@ def make_tables(contents):
     return tables
 
 
-def run(contents, reqs, max_inflight, sequential, max_batch_keys=0, packing=True, plain=False):
+def run(contents, reqs, max_inflight, sequential, max_batch_keys=0, packing=False, plain=False, direct=True):
     import b2co
     tables = make_tables(contents)
     srv = b2co.Server(max_inflight=max_inflight, hbm_budget_bytes=8 << 30, max_batch_keys=max_batch_keys)
     srv.set_packing(packing)
     srv.set_plain(plain)
+    srv.set_direct_results(direct)
     for m in tables:
         srv.register(m)
     ins, bufs, infos, ids = [], [], [], []
@@ -155,20 +156,22 @@ def test_results_same_alone_and_in_the_mix():
     assert b_stats["requests_launched"] == len(reqs)
     # staging was sized at creation: no buffer grew under traffic
     assert b_stats["staging_grows"] == 8
-    # coalesced launches shared one copy each way (packed), fewer copies than requests
-    assert b_stats["packed_launches"] > 0
-    assert b_stats["copies"] < a_stats["copies"]
+    # lookups took their results straight from the GPU: no copy out, so fewer copies than two per request
+    assert b_stats["direct_launches"] > 0 and a_stats["direct_launches"] > 0
+    assert b_stats["copies"] < 2 * len(reqs)
 
 
-def test_mix_unpacked_and_plain_modes_give_the_same_results():
-    """The coalescing server with per-request copies, and the plain baseline
-    (one launch per request, one request per table at a time), give the
-    sequential results too."""
+def test_mix_copied_packed_and_plain_modes_give_the_same_results():
+    """The coalescing server with results copied out per request, with
+    coalesced requests packed into one copy each way, and the plain baseline
+    (one launch per request, one request per table at a time; results copied
+    out or written directly) give the sequential results too."""
     import b2co
     contents = initial_contents()
     reqs = make_requests(contents)
     e_out = None
-    for kw in ({"packing": False}, {"plain": True}):
+    for kw in ({"direct": False}, {"direct": False, "packing": True}, {"plain": True, "direct": False},
+               {"plain": True}):
         out, info, pairs, stats, cap = run(contents, reqs, 8, sequential=False, **kw)
         if e_out is None:
             e_out, e_counts, e_pairs = expected(contents, reqs, cap)
@@ -179,7 +182,8 @@ def test_mix_unpacked_and_plain_modes_give_the_same_results():
                 assert (info[i].failed, info[i].assigned) == e_counts[i], (kw, i)
         for x, e in zip(pairs, e_pairs):
             assert np.array_equal(x, e), kw
-        assert stats["packed_launches"] == 0, kw
+        assert (stats["packed_launches"] > 0) == bool(kw.get("packing")), kw
+        assert (stats["direct_launches"] > 0) == kw.get("direct", True), kw
         if kw.get("plain"):
             assert stats["launches"] == len(reqs)
 
