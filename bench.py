@@ -1315,11 +1315,11 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
         log(f"[served] {rate} req/s: p50 {r['p50_ms']} ms, p99 {r['p99_ms']} ms, {r['gkeys_s']} Gkeys/s, "
             f"{r['requests_per_launch']} req/launch, {r['host_us_per_launch']} us host/launch")
         out.append(r)
-    # the same server with every result copied out per request, and with
-    # coalesced requests packed into one copy each way by host threads
-    srv.set_direct_results(False)
+    # the same server with lookup results written by the GPU into the pinned
+    # result buffers, and with coalesced requests packed into one copy each way
     copied, packed = [], []
-    for arm, lst in (("copied", copied), ("packed", packed)):
+    for arm, lst in (("direct", copied), ("packed", packed)):
+        srv.set_direct_results(arm == "direct")
         srv.set_packing(arm == "packed")
         for rate in rates:
             r = run_rate(rate, max(200, int(rate * seconds)))
@@ -1327,6 +1327,7 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
             lst.append({k: r[k] for k in ("offered_req_s", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
                                           "copies", "launches", "packed_launches")})
     srv.set_packing(False)
+    srv.set_direct_results(False)
     # the baseline on the same schedule: one plain launch per request, one
     # request per table at a time (copy in, Find / InsertOrAssign, copy out)
     srv.set_plain(True)
@@ -1336,9 +1337,9 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
         plain.append({k: r[k] for k in ("offered_req_s", "requests", "achieved_req_s", "gkeys_s", "p50_ms", "p99_ms",
                                         "launches")})
     srv.set_plain(False)
-    srv.set_direct_results(True)
     st = srv.stats()
     srv.close()
+    bus = copy_probe(in_arena, in_words, out_arena, ns)
     del tables
     torch.cuda.empty_cache()
     return {"served": {"tables": [int(x) for x in sizes], "table_gb": round(table_gb, 2), "load_factor": 0.6,
@@ -1346,9 +1347,42 @@ def served_measurements(stream, rates=SERVED_RATES, seconds=0.5, pool=384, infli
                        "request_pool": pool, "mean_request_keys": round(float(np.mean(ns)), 1),
                        "seconds_per_rate": seconds, "host_buffers": "pinned",
                        "staging_grows": st["staging_grows"], "max_loop_gap_us": round(st["max_loop_gap_ns"] / 1e3, 1),
-                       "sweep": out, "copied_results_sweep": copied, "packed_sweep": packed,
+                       "sweep": out, "direct_results_sweep": copied, "packed_sweep": packed,
                        "plain_per_table_sweep": plain,
-                       "server_over_plain_gkeys": [round(a["gkeys_s"] / b["gkeys_s"], 3) for a, b in zip(out, plain)]}}
+                       "server_over_plain_gkeys": [round(a["gkeys_s"] / b["gkeys_s"], 3) for a, b in zip(out, plain)],
+                       "copy_probe": bus}}
+
+
+def copy_probe(in_arena, in_words, out_arena, ns, streams=8, reps=3):
+    """What the bus moves for the served request sizes with no lookups at all:
+    every pool request's input copied in and a result of its size copied out,
+    back to back on `streams` streams; host to device only, device to host
+    only, and both at once (GB/s of payload each way, requests per second)."""
+    import torch
+    ss = [torch.cuda.Stream() for _ in range(streams)]
+    hin, hout, io, oo = [], [], 0, 0
+    for w, n in zip(in_words, ns):
+        hin.append(torch.from_numpy(in_arena[io:io + int(w)]))
+        hout.append(torch.from_numpy(out_arena[oo:oo + int(n)]))
+        io, oo = io + int(w), oo + int(n)
+    dev_in = torch.empty(int(in_words.max()), dtype=torch.int64, device="cuda")
+    dev_out = torch.empty(int(ns.max()), dtype=torch.int64, device="cuda")
+    res = {}
+    for name, h2d, d2h in (("h2d_only", True, False), ("d2h_only", False, True), ("both", True, True)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            for i in range(len(hin)):
+                with torch.cuda.stream(ss[i % streams]):
+                    if h2d:
+                        dev_in[:hin[i].numel()].copy_(hin[i], non_blocking=True)
+                    if d2h:
+                        hout[i].copy_(dev_out[:hout[i].numel()], non_blocking=True)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        moved = (float(in_words.sum()) if h2d else float(ns.sum())) * 8 * reps
+        res[name] = {"requests_per_s": round(reps * len(hin) / el), "gbs_each_way": round(moved / el / 1e9, 2)}
+    return res
 
 
 def run_reference(args):

@@ -367,12 +367,15 @@ int b2co_server_set_plain(b2co_server* server, int plain);
  * The arenas (24 bytes per key of a launch of up to 4 Mi keys, per slot) are
  * allocated with the server; larger launches copy per request. */
 int b2co_server_set_packing(b2co_server* server, int on);
-/* Direct results (on by default): a lookup launch whose requests' result
+/* Direct results (off by default): a lookup launch whose requests' result
  * buffers are pinned host memory gets its results written into them by the
  * GPU (one small kernel of SM stores over PCIe per launch) instead of one
  * device-to-host copy per request, so a lookup costs the copy engines one
  * operation, its keys in.  Requests with pageable result buffers are copied
- * as before.  In plain mode the same applies per request. */
+ * as before.  In plain mode the same applies per request.  Measured on the
+ * served benchmark it moves the same bytes over the same bus, so throughput
+ * is unchanged; it is off by default because its extra kernel per launch
+ * raised p99 latency at moderate rates. */
 int b2co_server_set_direct_results(b2co_server* server, int on);
 /* host_in: keys (Find/Contains) or pairs (Insert/InsertOrAssign); host_out:
  * payloads (Find) or 1-byte flags (Contains), unused otherwise. */

@@ -550,7 +550,7 @@ class Server:
         _call("b2co_server_set_packing", self._h, C.c_int(1 if on else 0))
 
     def set_direct_results(self, on: bool):
-        """Lookup results written by the GPU into pinned host buffers (on by default)."""
+        """Lookup results written by the GPU into pinned host buffers (off by default)."""
         _call("b2co_server_set_direct_results", self._h, C.c_int(1 if on else 0))
 
     def set_plain(self, plain: bool):

@@ -317,7 +317,11 @@ __global__ void __launch_bounds__(256, kWriteMinBlocks<Q>) k_insert_win(__grid_c
         }
     };
 
-    // the next pass's pairs are loaded one pass ahead
+    // the next pass's pairs are loaded one pass ahead (B2CO_WRITE_PREFETCH 0:
+    // at the start of their own pass)
+#ifndef B2CO_WRITE_PREFETCH
+#define B2CO_WRITE_PREFETCH 1
+#endif
     Raw nxt[Q];
     bool nin[Q];
     auto load_pass = [&](uint32_t base) {
@@ -328,8 +332,9 @@ __global__ void __launch_bounds__(256, kWriteMinBlocks<Q>) k_insert_win(__grid_c
             nxt[q] = nin[q] ? Io<S>::load_pair(pairs, i) : Raw{};
         }
     };
-    load_pass(gwarp * PASS);
+    if (B2CO_WRITE_PREFETCH) load_pass(gwarp * PASS);
     for (uint32_t base = gwarp * PASS; base < n; base += nwarps * PASS) {
+        if (!B2CO_WRITE_PREFETCH) load_pass(base);
         Raw pr[Q];
         uint32_t idx[Q];
         int state[Q];
@@ -341,7 +346,7 @@ __global__ void __launch_bounds__(256, kWriteMinBlocks<Q>) k_insert_win(__grid_c
             state[q] = !nin[q] ? kWinIdle : (key == a.empty_key ? kWinSettled : kWinOpen);
             if (int(r) == q && state[q] == kWinOpen) my_init = probe_init<S::key_bytes, B>(a.probe, key);
         }
-        load_pass(base + nwarps * PASS);
+        if (B2CO_WRITE_PREFETCH) load_pass(base + nwarps * PASS);
         Raw w[Q][ROUNDS];
 #pragma unroll
         for (int q = 0; q < Q; ++q) {

@@ -223,7 +223,7 @@ struct b2co_server {
     // arenas exist from creation; `pack` switches their use on and off
     std::unique_ptr<CopyPool> packer;
     std::atomic<bool> pack{false};
-    std::atomic<bool> direct{true};  // lookups write results straight into pinned host buffers
+    std::atomic<bool> direct{false};  // lookups write results straight into pinned host buffers
     std::atomic<uint64_t> packed_launches{0}, direct_launches{0};
 
     // submission side (in_mu)

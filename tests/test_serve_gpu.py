@@ -97,6 +97,9 @@ def make_tables(contents):
 
 
 def run(contents, reqs, max_inflight, sequential, max_batch_keys=0, packing=False, plain=False, direct=True):
+    """Runs the requests through a server; `direct` (results written by the
+    GPU into the pinned result buffers) is on here so the default test covers
+    that path, the other modes are switched explicitly."""
     import b2co
     tables = make_tables(contents)
     srv = b2co.Server(max_inflight=max_inflight, hbm_budget_bytes=8 << 30, max_batch_keys=max_batch_keys)
