@@ -23,7 +23,8 @@
 #include "b2co_host.h"
 
 int b2co_oa_iaf_first_wins_on(b2co_oa_table* t, void const* pairs, void* out_found, uint8_t* out_inserted, uint64_t n,
-                              uint32_t* pos, uint32_t* newbits, uint32_t* owner, cudaStream_t s);
+                              uint32_t* pos, uint32_t* newbits, uint32_t* owner, bool owner_clear,
+                              cudaStream_t s);
 
 namespace {
 
@@ -71,7 +72,9 @@ int b2co_oa_insert_and_find_noalloc(b2co_oa_table* t, void const* pairs, void* o
     auto* newbits = reinterpret_cast<uint32_t*>(bytes + pos_bytes);
     auto* owner = reinterpret_cast<uint32_t*>(bytes + pos_bytes + bits_bytes);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    if (int st = b2co_oa_iaf_first_wins_on(t, pairs, out_found, out_inserted, n, pos, newbits, owner, s)) return st;
+    // the owner entries move with n inside the shared area, so they are set on every call
+    if (int st = b2co_oa_iaf_first_wins_on(t, pairs, out_found, out_inserted, n, pos, newbits, owner, false, s))
+        return st;
     B2CO_CUDA(cudaStreamSynchronize(s));
     return B2CO_OK;
 }

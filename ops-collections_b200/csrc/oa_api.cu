@@ -145,8 +145,11 @@ int ensure_first_wins_scratch(b2co_oa_table* t, uint64_t n)
 {
     if (!t->d_newbits) {
         uint64_t words = (t->capacity + 31) / 32;
-        B2CO_CUDA(cudaMalloc(&t->d_newbits, 2 * words * 4));  // claimed bits, then lowered bits
+        B2CO_CUDA(cudaMalloc(&t->d_newbits, 2 * words * 4));  // claimed bits, then shared bits
         B2CO_CUDA(cudaMalloc(&t->d_owner, t->capacity * 4));
+        // owner entries stay all-ones between batches (each batch restores the ones it used)
+        B2CO_CUDA(cudaMemset(t->d_owner, 0xff, t->capacity * 4));
+        B2CO_CUDA(cudaStreamSynchronize(nullptr));  // done before any stream of the caller's uses it
     }
     if (t->pos_cap < n) {
         if (t->d_pos) cudaFree(t->d_pos);
@@ -160,14 +163,17 @@ int ensure_first_wins_scratch(b2co_oa_table* t, uint64_t n)
 
 }  // namespace
 
-// First-wins InsertAndFind on scratch the caller provides: pos[n],
-// newbits[ceil(capacity/32)] (cleared here) and owner[capacity].
+// First-wins InsertAndFind on scratch the caller provides: pos[n], two
+// bitmaps of ceil(capacity/32) words (cleared here) and owner[capacity], whose
+// entries must be all-ones on entry unless `owner_clear` is false (then they
+// are set here); the call leaves them all-ones.
 int b2co_oa_iaf_first_wins_on(b2co_oa_table* t, void const* pairs, void* out_found, uint8_t* out_inserted, uint64_t n,
-                              uint32_t* pos, uint32_t* newbits, uint32_t* owner, cudaStream_t s)
+                              uint32_t* pos, uint32_t* newbits, uint32_t* owner, bool owner_clear, cudaStream_t s)
 {
     if (int st = check_table(t)) return st;
     if (int st = check_batch(n)) return st;
     B2CO_CUDA(cudaMemsetAsync(newbits, 0, ((t->capacity + 31) / 32) * 8, s));
+    if (!owner_clear) B2CO_CUDA(cudaMemsetAsync(owner, 0xff, t->capacity * 4, s));
     return t->ops->iaf_first(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), pos, newbits,
                              owner, s);
 }

@@ -41,7 +41,7 @@ struct InsOut {
     uint8_t* inserted;             // race: 1 = this input inserted the key
     uint32_t* pos;                 // place: slot of every input (kNoSlot = failed)
     uint32_t* newbits;             // place: slots claimed by this batch
-    uint32_t* owner;               // place: claiming input of each claimed slot
+    uint32_t* owner;               // place: claiming input of each claimed slot (claim_bit 0 only)
     uint32_t claim_bit;            // place: flag OR-ed into pos[] of the claiming input (0 = none)
 };
 
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(256, kWriteMinBlocks<Q>) k_insert_win(__grid_c
             uint32_t const p = verdict == kFailed ? kNoSlot : where;
             if (verdict == kSuccess) {
                 atomicOr(o.newbits + (p >> 5), 1u << (p & 31));
-                o.owner[p] = i;
+                if (!o.claim_bit) o.owner[p] = i;  // tables without room for the claim bit
             }
             o.pos[i] = verdict == kSuccess ? (p | o.claim_bit) : p;
         }

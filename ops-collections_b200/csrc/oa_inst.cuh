@@ -124,8 +124,8 @@ struct OaImpl {
         return with_b(b, [&](auto bc) {
             constexpr int B = decltype(bc)::value;
             // `newbits` holds two bitmaps of the table's slots: claimed in this
-            // batch, then lowered (a smaller input index than the claimer's)
-            uint32_t* lowered = newbits + (uint64_t(a.probe.capacity) + 31) / 32;
+            // batch, then shared with later inputs of the batch (`dup`)
+            uint32_t* dup = newbits + (uint64_t(a.probe.capacity) + 31) / 32;
             uint32_t const claim_bit = a.probe.capacity < kClaimBit ? kClaimBit : 0u;  // slot indices below 2^31 - 1
             bool placed = false;
             if constexpr (B > 1) {
@@ -144,12 +144,15 @@ struct OaImpl {
                 k1<<<grid_for((void const*)k1, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, n, pos, newbits, owner,
                                                                                     claim_bit);
             }
-            auto k2 = k_iaf_min<S>;
-            k2<<<grid_for((void const*)k2, kBlock, n, kBlock), kBlock, 0, s>>>(pos, newbits, lowered, owner, n,
-                                                                                claim_bit);
+            auto const grid = [&](void const* k) { return grid_for(k, kBlock, n, kBlock); };
+            k_iaf_min<S><<<grid((void const*)k_iaf_min<S>), kBlock, 0, s>>>(pos, newbits, dup, owner, n, claim_bit);
+            if (claim_bit)
+                k_iaf_claim<S><<<grid((void const*)k_iaf_claim<S>), kBlock, 0, s>>>(pos, dup, owner, n, claim_bit);
             auto k3 = k_iaf_final<S>;
-            k3<<<grid_for((void const*)k3, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, pos, newbits, lowered, owner,
-                                                                                found, inserted, n, claim_bit);
+            k3<<<grid((void const*)k3), kBlock, 0, s>>>(a, pairs, pos, newbits, dup, owner, found, inserted, n,
+                                                        claim_bit);
+            if (claim_bit)
+                k_iaf_restore<S><<<grid((void const*)k_iaf_restore<S>), kBlock, 0, s>>>(pos, dup, owner, n, claim_bit);
             return check_launch("insert_and_find (first wins) kernels");
         });
     }

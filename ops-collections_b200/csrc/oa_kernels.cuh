@@ -291,23 +291,33 @@ __global__ void __launch_bounds__(256) k_iaf_race(__grid_constant__ const OaArgs
 // ----------------------------------------------------------------------------
 // InsertAndFind, first-wins mode: deterministic, equal to inserting the batch
 // sequentially in input order (the golden of tests/common/golden.h:104-131).
-//   place : every key finds or claims its slot; pos[i] = slot; a claiming
-//           thread marks the slot new and records itself as its owner;
-//   min   : the other inputs on a new slot lower the owner to the least
-//           input index (atomicMin) and, when they did lower it, set the
-//           slot's bit in `lowered`;
-//   final : owner i is the inserted one; every other input on a new slot
-//           finds the owner's payload (read from the input, never a racing
-//           slot); inputs on old slots find the stored payload.
-// When the table has at most 2^31 slots, pos[i] of the input that claimed the
-// slot carries kClaimBit: min skips the claimers, and in final a claimer whose
-// slot was not lowered is the inserted one without reading owner[] and
-// without rewriting a slot its CAS already filled -- the common case costs
-// no random DRAM access after placement.  `lowered` is the bitmap right after
-// `newbits` (both cleared before place).
+// When the table has fewer than 2^31 slots, pos[i] of the input that claimed a
+// slot carries kClaimBit, and owner[] (one entry per slot) holds kNoOwner
+// between batches:
+//   place   : every key finds or claims its slot; pos[i] = slot; a claimer
+//             marks the slot in `newbits` (claimed by this batch) and writes
+//             nothing else -- a unique key costs no random access besides its
+//             window and its CAS;
+//   min     : the other inputs on a claimed slot lower owner[slot] to the
+//             least of their indices (atomicMin); the first of them marks the
+//             slot in `dup`;
+//   claim   : the claimer of a slot in `dup` lowers owner[slot] to its own
+//             index when smaller;
+//   final   : a claimer whose slot is not in `dup` is the inserted input (its
+//             CAS stored its pair); on a slot in `dup` the input owner[slot]
+//             names is the inserted one, every input there finds that input's
+//             payload (read from the inputs, never a racing slot), and an owner
+//             that was not the claimer rewrites the payload; inputs on older
+//             slots find the stored payload;
+//   restore : the claimers of slots in `dup` put owner[slot] back to kNoOwner.
+// Tables of 2^31 slots or more have no room for the claim bit in pos[]: there
+// the claimer writes owner[slot] in place, min lowers it over every input on
+// the slot, final reads it for all of them, and claim and restore do not run.
+// `dup` is the bitmap right after `newbits` (both cleared before place).
 // ----------------------------------------------------------------------------
 
 constexpr uint32_t kClaimBit = 0x80000000u;
+constexpr uint32_t kNoOwner = 0xffffffffu;
 
 template <class S, int B>
 __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArgs a, void const* pairs, uint32_t n, uint32_t* pos,
@@ -340,7 +350,7 @@ __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArg
                         if (raw_eq(old, expected)) {
                             where = idx + j;
                             atomicOr(newbits + (where >> 5), 1u << (where & 31));
-                            owner[where] = i;
+                            if (!claim_bit) owner[where] = i;
                             where |= claim_bit;
                             done = true;
                         } else if (S::key_eq(S::key(old), key)) {
@@ -362,7 +372,7 @@ __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArg
 __device__ __forceinline__ bool bit_set(uint32_t const* bits, uint32_t s) { return (bits[s >> 5] >> (s & 31)) & 1u; }
 
 template <class S>  // one copy per slot layout's translation unit
-__global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t const* newbits, uint32_t* lowered,
+__global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t const* newbits, uint32_t* dup,
                                                  uint32_t* owner, uint32_t n, uint32_t claim_bit)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -371,13 +381,37 @@ __global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t c
         uint32_t const s = p & ~claim_bit;
         if (!bit_set(newbits, s)) continue;
         uint32_t const was = atomicMin(owner + s, i);
-        if (i < was) atomicOr(lowered + (s >> 5), 1u << (s & 31));
+        if (claim_bit && was == kNoOwner) atomicOr(dup + (s >> 5), 1u << (s & 31));
+    }
+}
+
+template <class S>  // the claimer is the only writer of its slot's owner entry in this launch
+__global__ void __launch_bounds__(256) k_iaf_claim(uint32_t const* pos, uint32_t const* dup, uint32_t* owner,
+                                                   uint32_t n, uint32_t claim_bit)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t const p = pos[i];
+        if (p == kNoSlot || !(p & claim_bit)) continue;
+        uint32_t const s = p & ~claim_bit;
+        if (bit_set(dup, s) && i < owner[s]) owner[s] = i;
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(256) k_iaf_restore(uint32_t const* pos, uint32_t const* dup, uint32_t* owner,
+                                                     uint32_t n, uint32_t claim_bit)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t const p = pos[i];
+        if (p == kNoSlot || !(p & claim_bit)) continue;
+        uint32_t const s = p & ~claim_bit;
+        if (bit_set(dup, s)) owner[s] = kNoOwner;
     }
 }
 
 template <class S>
 __global__ void __launch_bounds__(256) k_iaf_final(__grid_constant__ const OaArgs a, void const* pairs, uint32_t const* pos,
-                                                   uint32_t const* newbits, uint32_t const* lowered,
+                                                   uint32_t const* newbits, uint32_t const* dup,
                                                    uint32_t const* owner, void* out_found, uint8_t* out_inserted,
                                                    uint32_t n, uint32_t claim_bit)
 {
@@ -390,7 +424,7 @@ __global__ void __launch_bounds__(256) k_iaf_final(__grid_constant__ const OaArg
         if (p != kNoSlot) {
             bool const claimed = (p & claim_bit) != 0;
             uint32_t const s = p & ~claim_bit;
-            if (claimed && !bit_set(lowered, s)) {  // the claimer is the least index: its CAS stored its pair
+            if (claimed && !bit_set(dup, s)) {  // the claimer alone: its CAS stored its pair
                 inserted = 1;
                 found = S::value(Io<S>::load_pair(pairs, i));
             } else if (bit_set(newbits, s)) {
