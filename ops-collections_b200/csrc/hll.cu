@@ -6,9 +6,9 @@
 // rank).  Registers are bytes, register i at byte i (four per 32-bit word).
 //
 // B200 design: Add keeps a private copy of the registers in shared memory
-// (p <= 17: 8..128 KiB per CTA), reads each key once from HBM, and raises a
-// shared register with a compare-and-swap loop only when the new rank is
-// larger (after warm-up almost never).  Each CTA then folds its copy into the
+// (p <= 17: 8..128 KiB per CTA of 1024 threads), reads each key once from HBM
+// in 16-byte loads, and raises a shared register with a compare-and-swap loop
+// only when the new rank is larger (after warm-up almost never).  Each CTA then folds its copy into the
 // global registers with a per-byte max (__vmaxu4) CAS on words that changed.
 // p = 18 (256 KiB) exceeds shared memory and updates the global registers
 // directly, with the same read-before-CAS filter.  Estimate builds the 65-bin
@@ -70,36 +70,68 @@ __device__ __forceinline__ void fold_word(uint32_t* g, uint32_t mine)
     }
 }
 
-template <int KB>
-__global__ void __launch_bounds__(512) k_hll_add_shared(uint32_t* regs, uint32_t p, void const* keys, uint64_t n)
+// Precision as a compile-time constant: the index and rank shifts become
+// immediates.
+template <int KB, int P>
+__device__ __forceinline__ void hll_locate_p(uint64_t key, uint32_t& index, uint32_t& rank)
+{
+    uint64_t const h = xxh64<KB>(key, 0);
+    index = uint32_t(h >> (64 - P));
+    rank = uint32_t(__clzll((long long)((h << P) | (1ull << (P - 1))))) + 1u;
+}
+
+constexpr int kHllBlock = 1024;
+
+// Add for p <= 17 with 16-byte key loads: a CTA of 1024 threads keeps one
+// private register copy (2^P bytes of shared memory), so at p = 16 two CTAs
+// fill an SM's 64 warps.  Keys before the first 16-byte boundary (`head`) and
+// after the last whole vector go one per thread.
+template <int KB, int P>
+__global__ void __launch_bounds__(kHllBlock, P <= 16 ? 2 : 1)
+    k_hll_add_vec(uint32_t* regs, void const* keys, uint64_t n, uint64_t head)
 {
     extern __shared__ uint32_t sk[];
-    uint32_t const words = (1u << p) / 4;
-    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) sk[i] = 0;
+    constexpr uint32_t kWords = (1u << P) / 4;
+    constexpr int V = 16 / KB;        // keys per 16-byte load
+    constexpr int U = KB == 8 ? 2 : 1;  // loads in flight per thread
+    for (uint32_t i = threadIdx.x; i < kWords; i += kHllBlock) sk[i] = 0;
     __syncthreads();
-    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
-    uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    // kItems keys per iteration keep as many independent load-and-hash chains in
-    // flight (the sketch's shared memory, not registers, limits the CTAs per SM)
-    constexpr int kItems = 4;
-    for (; i + (kItems - 1) * stride < n; i += kItems * stride) {
-        uint64_t k[kItems];
-#pragma unroll
-        for (int j = 0; j < kItems; ++j) k[j] = load_key<KB>(keys, i + j * stride);
-        uint32_t x[kItems], r[kItems];
-#pragma unroll
-        for (int j = 0; j < kItems; ++j) hll_locate<KB>(k[j], p, x[j], r[j]);
-#pragma unroll
-        for (int j = 0; j < kItems; ++j) raise_register(sk, x[j], r[j]);
-    }
-    for (; i < n; i += stride) {
+    uint64_t const tid = uint64_t(blockIdx.x) * kHllBlock + threadIdx.x;
+    uint64_t const stride = uint64_t(gridDim.x) * kHllBlock;
+    auto add = [&](uint64_t key) {
         uint32_t x, r;
-        hll_locate<KB>(load_key<KB>(keys, i), p, x, r);
-        raise_register(sk, x, r);
+        hll_locate_p<KB, P>(key, x, r);
+        raise_register(sk, x, r);  // a word load decides; a byte load measured 3.5x slower
+    };
+    uint64_t const body = head < n ? n - head : 0;
+    uint64_t const nvec = body / V;
+    uint64_t const tail0 = head + nvec * V;
+    for (uint64_t i = tid; i < head && i < n; i += stride) add(load_key<KB>(keys, i));
+    for (uint64_t i = tail0 + tid; i < n; i += stride) add(load_key<KB>(keys, i));
+    uint4 const* vk = reinterpret_cast<uint4 const*>(static_cast<char const*>(keys) + head * KB);
+    auto add_vec = [&](uint4 q) {
+        if constexpr (KB == 8) {
+            add(uint64_t(q.x) | (uint64_t(q.y) << 32));
+            add(uint64_t(q.z) | (uint64_t(q.w) << 32));
+        } else {
+            add(q.x);
+            add(q.y);
+            add(q.z);
+            add(q.w);
+        }
+    };
+    uint64_t v = tid;
+    for (; v + (U - 1) * stride < nvec; v += U * stride) {
+        uint4 q[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) q[j] = __ldcs(vk + v + j * stride);
+#pragma unroll
+        for (int j = 0; j < U; ++j) add_vec(q[j]);
     }
+    for (; v < nvec; v += stride) add_vec(__ldcs(vk + v));
     __syncthreads();
-    for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
-        uint32_t mine = sk[w];
+    for (uint32_t w = threadIdx.x; w < kWords; w += kHllBlock) {
+        uint32_t const mine = sk[w];
         if (mine) fold_word(regs + w, mine);
     }
 }
@@ -261,22 +293,29 @@ int add_launch(b2co_hll* h, void const* keys, uint64_t n, cudaStream_t s)
 {
     uint32_t const p = h->precision;
     if (p <= 17) {
-        size_t smem = size_t(1) << p;
-        void (*k)(uint32_t*, uint32_t, void const*, uint64_t) =
-            h->key_bytes == 8 ? k_hll_add_shared<8> : k_hll_add_shared<4>;
-        static bool attr_set[2] = {false, false};
-        int const ki = h->key_bytes == 8;
-        if (!attr_set[ki]) {
-            B2CO_CUDA(cudaFuncSetAttribute((void const*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
-            attr_set[ki] = true;
+        using AddFn = void (*)(uint32_t*, void const*, uint64_t, uint64_t);
+        static AddFn const fns[2][5] = {
+            {k_hll_add_vec<4, 13>, k_hll_add_vec<4, 14>, k_hll_add_vec<4, 15>, k_hll_add_vec<4, 16>,
+             k_hll_add_vec<4, 17>},
+            {k_hll_add_vec<8, 13>, k_hll_add_vec<8, 14>, k_hll_add_vec<8, 15>, k_hll_add_vec<8, 16>,
+             k_hll_add_vec<8, 17>}};
+        static int per_sm_cache[2][5] = {};
+        int const ki = h->key_bytes == 8, pi = int(p) - 13;
+        AddFn const k = fns[ki][pi];
+        size_t const smem = size_t(1) << p;
+        if (!per_sm_cache[ki][pi]) {
+            B2CO_CUDA(cudaFuncSetAttribute((void const*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+            int per_sm = 0;
+            B2CO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)k, kHllBlock, smem));
+            per_sm_cache[ki][pi] = per_sm < 1 ? 1 : per_sm;
         }
-        int per_sm = 0;
-        B2CO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)k, 512, smem));
-        if (per_sm < 1) per_sm = 1;
-        uint64_t want = (n + 512 * 16 - 1) / (512 * 16);  // at least ~16 keys per thread
-        uint64_t cap = uint64_t(per_sm) * sm_count();
-        uint32_t grid = uint32_t(want < 1 ? 1 : (want < cap ? want : cap));
-        k<<<grid, 512, smem, s>>>(h->regs, p, keys, n);
+        uint64_t const want = (n + uint64_t(kHllBlock) * 16 - 1) / (uint64_t(kHllBlock) * 16);  // >= ~16 keys a thread
+        uint64_t const cap = uint64_t(per_sm_cache[ki][pi]) * sm_count();
+        uint32_t const grid = uint32_t(want < 1 ? 1 : (want < cap ? want : cap));
+        // keys up to the first 16-byte boundary go one per thread
+        uintptr_t const addr = reinterpret_cast<uintptr_t>(keys);
+        uint64_t const head = ((16 - addr % 16) % 16) / h->key_bytes;
+        k<<<grid, kHllBlock, smem, s>>>(h->regs, keys, n, head);
     } else {
         void (*k)(uint32_t*, uint32_t, void const*, uint64_t) =
             h->key_bytes == 8 ? k_hll_add_global<8> : k_hll_add_global<4>;

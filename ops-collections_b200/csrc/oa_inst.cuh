@@ -144,15 +144,25 @@ struct OaImpl {
                 k1<<<grid_for((void const*)k1, kBlock, n, kBlock), kBlock, 0, s>>>(a, pairs, n, pos, newbits, owner,
                                                                                     claim_bit);
             }
-            auto const grid = [&](void const* k) { return grid_for(k, kBlock, n, kBlock); };
+            auto const grid = [&](void const* k) { return grid_for(k, kBlock, (uint64_t(n) + 3) / 4, kBlock); };
             k_iaf_min<S><<<grid((void const*)k_iaf_min<S>), kBlock, 0, s>>>(pos, newbits, dup, owner, n, claim_bit);
             if (claim_bit)
                 k_iaf_claim<S><<<grid((void const*)k_iaf_claim<S>), kBlock, 0, s>>>(pos, dup, owner, n, claim_bit);
             auto k3 = k_iaf_final<S>;
             k3<<<grid((void const*)k3), kBlock, 0, s>>>(a, pairs, pos, newbits, dup, owner, found, inserted, n,
                                                         claim_bit);
-            if (claim_bit)
-                k_iaf_restore<S><<<grid((void const*)k_iaf_restore<S>), kBlock, 0, s>>>(pos, dup, owner, n, claim_bit);
+            if (claim_bit) {
+                // owner[] back to all-ones: a batch within 8x of the table's slots
+                // clears the whole array (one sequential write) rather than
+                // visiting its shared slots at random
+                if (uint64_t(a.probe.capacity) <= 8ull * n) {
+                    cudaError_t const e = cudaMemsetAsync(owner, 0xff, uint64_t(a.probe.capacity) * 4, s);
+                    if (e != cudaSuccess) return cuda_fail(e, "insert_and_find (first wins) owner reset");
+                } else {
+                    k_iaf_restore<S><<<grid((void const*)k_iaf_restore<S>), kBlock, 0, s>>>(pos, dup, owner, n,
+                                                                                             claim_bit);
+                }
+            }
             return check_launch("insert_and_find (first wins) kernels");
         });
     }
@@ -365,8 +375,10 @@ struct GroupImpl {
 
     // `shape` packs lanes per window (bits 0-7), keys in flight per lane group
     // (bits 8-15; 1 = one key per tile, resolved at once) and threads per block
-    // (bits 16-31; 0 = 256).  Keys per tile above 1 run the deferred kernel;
-    // its 2-, 4- and 8-lane variants other than 4x2 exist for bucket size 5.
+    // (bits 16-31; 0 = 256).  With 2 or more lanes, keys per tile above 1 run
+    // the deferred kernel; its 2-, 4- and 8-lane variants other than 4x2 exist
+    // for bucket size 5.  With one lane, 2 or 4 keys per tile are the keys a
+    // lane loads before it scans (bucket size 5; otherwise 1).
     template <int B, bool C>
     static int find_b(GroupArgs const& g, uint32_t shape, void const* keys, void* out, uint64_t n, cudaStream_t s)
     {
@@ -382,6 +394,10 @@ struct GroupImpl {
             if (!k) k = k_group_find_q<S, B, 4, 2, C>;
         } else if (lanes <= 1) {
             k = k_group_find<S, B, 1, C>;
+            if constexpr (B == 5) {
+                if (items == 2) k = k_group_find<S, B, 1, C, 2>;
+                else if (items >= 4) k = k_group_find<S, B, 1, C, 4>;
+            }
         } else if (lanes == 2) {
             k = k_group_find<S, B, 2, C>;
         } else if (lanes == 4) {

@@ -371,41 +371,93 @@ __global__ void __launch_bounds__(256) k_iaf_place(__grid_constant__ const OaArg
 
 __device__ __forceinline__ bool bit_set(uint32_t const* bits, uint32_t s) { return (bits[s >> 5] >> (s & 31)) & 1u; }
 
+// The passes after placement take four inputs a thread: one 16-byte load of
+// their pos[] entries, then each dependent step (bitmap word, owner entry,
+// input pair) issued for all four before any is used, so a thread keeps four
+// independent chains of loads in flight.
+constexpr uint32_t kIafItems = 4;
+
+__device__ __forceinline__ void load_pos4(uint32_t const* pos, uint32_t n, uint32_t i0, uint32_t (&p)[kIafItems])
+{
+    if (i0 + kIafItems <= n) {
+        uint4 const v = __ldcs(reinterpret_cast<uint4 const*>(pos + i0));  // pos[] is 16-byte aligned
+        p[0] = v.x, p[1] = v.y, p[2] = v.z, p[3] = v.w;
+    } else {
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k) p[k] = i0 + k < n ? pos[i0 + k] : kNoSlot;
+    }
+}
+
+__device__ __forceinline__ bool bit_of(uint32_t word, uint32_t s) { return (word >> (s & 31)) & 1u; }
+
 template <class S>  // one copy per slot layout's translation unit
 __global__ void __launch_bounds__(256) k_iaf_min(uint32_t const* pos, uint32_t const* newbits, uint32_t* dup,
                                                  uint32_t* owner, uint32_t n, uint32_t claim_bit)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t const p = pos[i];
-        if (p == kNoSlot || (p & claim_bit)) continue;  // failed, or the claimer itself
-        uint32_t const s = p & ~claim_bit;
-        if (!bit_set(newbits, s)) continue;
-        uint32_t const was = atomicMin(owner + s, i);
-        if (claim_bit && was == kNoOwner) atomicOr(dup + (s >> 5), 1u << (s & 31));
+    uint32_t const groups = (n + kIafItems - 1) / kIafItems;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+        uint32_t const i0 = q * kIafItems;
+        uint32_t p[kIafItems], w[kIafItems];
+        load_pos4(pos, n, i0, p);
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k)  // failed inputs and the claimers themselves skip
+            w[k] = p[k] != kNoSlot && !(p[k] & claim_bit) ? newbits[(p[k] & ~claim_bit) >> 5] : 0u;
+        uint32_t was[kIafItems];
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k) {
+            uint32_t const sl = p[k] & ~claim_bit;
+            was[k] = w[k] && bit_of(w[k], sl) ? atomicMin(owner + sl, i0 + k) : 0u;
+        }
+        if (claim_bit) {
+#pragma unroll
+            for (uint32_t k = 0; k < kIafItems; ++k) {
+                uint32_t const sl = p[k] & ~claim_bit;
+                if (w[k] && bit_of(w[k], sl) && was[k] == kNoOwner) atomicOr(dup + (sl >> 5), 1u << (sl & 31));
+            }
+        }
     }
 }
 
-template <class S>  // the claimer is the only writer of its slot's owner entry in this launch
+// The claimer of a slot in `dup` is the only writer of its owner entry in this
+// launch.
+template <class S>
 __global__ void __launch_bounds__(256) k_iaf_claim(uint32_t const* pos, uint32_t const* dup, uint32_t* owner,
                                                    uint32_t n, uint32_t claim_bit)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t const p = pos[i];
-        if (p == kNoSlot || !(p & claim_bit)) continue;
-        uint32_t const s = p & ~claim_bit;
-        if (bit_set(dup, s) && i < owner[s]) owner[s] = i;
+    uint32_t const groups = (n + kIafItems - 1) / kIafItems;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+        uint32_t const i0 = q * kIafItems;
+        uint32_t p[kIafItems], w[kIafItems], o[kIafItems];
+        load_pos4(pos, n, i0, p);
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k)
+            w[k] = p[k] != kNoSlot && (p[k] & claim_bit) ? dup[(p[k] & ~claim_bit) >> 5] : 0u;
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k)
+            o[k] = w[k] && bit_of(w[k], p[k] & ~claim_bit) ? owner[p[k] & ~claim_bit] : 0u;
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k)
+            if (w[k] && bit_of(w[k], p[k] & ~claim_bit) && i0 + k < o[k]) owner[p[k] & ~claim_bit] = i0 + k;
     }
 }
 
+// Puts owner[] back to all-ones on the slots in `dup` (batches small against
+// the table; a large one clears the whole array instead).
 template <class S>
 __global__ void __launch_bounds__(256) k_iaf_restore(uint32_t const* pos, uint32_t const* dup, uint32_t* owner,
                                                      uint32_t n, uint32_t claim_bit)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t const p = pos[i];
-        if (p == kNoSlot || !(p & claim_bit)) continue;
-        uint32_t const s = p & ~claim_bit;
-        if (bit_set(dup, s)) owner[s] = kNoOwner;
+    uint32_t const groups = (n + kIafItems - 1) / kIafItems;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+        uint32_t const i0 = q * kIafItems;
+        uint32_t p[kIafItems], w[kIafItems];
+        load_pos4(pos, n, i0, p);
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k)
+            w[k] = p[k] != kNoSlot && (p[k] & claim_bit) ? dup[(p[k] & ~claim_bit) >> 5] : 0u;
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k)
+            if (w[k] && bit_of(w[k], p[k] & ~claim_bit)) owner[p[k] & ~claim_bit] = kNoOwner;
     }
 }
 
@@ -417,30 +469,58 @@ __global__ void __launch_bounds__(256) k_iaf_final(__grid_constant__ const OaArg
 {
     using Raw = typename S::Raw;
     Raw* slots = reinterpret_cast<Raw*>(a.slots);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t const p = pos[i];
-        uint64_t found = empty_payload<S>(a);
-        uint8_t inserted = 0;
-        if (p != kNoSlot) {
-            bool const claimed = (p & claim_bit) != 0;
-            uint32_t const s = p & ~claim_bit;
-            if (claimed && !bit_set(dup, s)) {  // the claimer alone: its CAS stored its pair
-                inserted = 1;
-                found = S::value(Io<S>::load_pair(pairs, i));
-            } else if (bit_set(newbits, s)) {
-                uint32_t m = owner[s];
-                Raw pm = Io<S>::load_pair(pairs, m);
-                found = S::value(pm);
-                if (m == i) {
-                    inserted = 1;
-                    if (!claimed) assign_payload<S>(slots + s, S::key(pm), found);
-                }
-            } else {
-                found = S::value(ld_rw(slots + s));
-            }
+    enum : uint32_t { kNone, kAlone, kShared, kOld };
+    uint32_t const groups = (n + kIafItems - 1) / kIafItems;
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < groups; q += gridDim.x * blockDim.x) {
+        uint32_t const i0 = q * kIafItems;
+        uint32_t p[kIafItems], w[kIafItems], kind[kIafItems], m[kIafItems];
+        load_pos4(pos, n, i0, p);
+        // a claimer reads its dup bit, any other input the claimed bit of its slot
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k) {
+            uint32_t const sl = p[k] & ~claim_bit;
+            w[k] = p[k] == kNoSlot ? 0u : (p[k] & claim_bit) ? dup[sl >> 5] : newbits[sl >> 5];
         }
-        Io<S>::store_payload(out_found, i, found);
-        out_inserted[i] = inserted;
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k) {
+            uint32_t const sl = p[k] & ~claim_bit;
+            bool const claimed = p[k] != kNoSlot && (p[k] & claim_bit);
+            // a claimer alone on its slot: its CAS stored its pair.  Otherwise a
+            // slot claimed by this batch names its inserted input in owner[]
+            // (claimers reach this only through dup), and an older slot holds
+            // the payload to find.
+            kind[k] = p[k] == kNoSlot ? kNone
+                      : claimed       ? (bit_of(w[k], sl) ? kShared : kAlone)
+                                      : (bit_of(w[k], sl) ? kShared : kOld);
+        }
+        Raw v[kIafItems];
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k) {
+            uint32_t const sl = p[k] & ~claim_bit;
+            m[k] = kind[k] == kShared ? owner[sl] : i0 + k;
+            if (kind[k] == kOld) v[k] = ld_rw(slots + sl);
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k)
+            if (kind[k] == kAlone || kind[k] == kShared) v[k] = Io<S>::load_pair(pairs, m[k]);
+#pragma unroll
+        for (uint32_t k = 0; k < kIafItems; ++k) {
+            uint32_t const i = i0 + k;
+            if (i >= n) break;
+            uint64_t found = empty_payload<S>(a);
+            uint8_t inserted = 0;
+            if (kind[k] != kNone) {
+                found = S::value(v[k]);
+                if (kind[k] == kAlone || (kind[k] == kShared && m[k] == i)) {
+                    inserted = 1;
+                    // an owner that is not the claimer rewrites the payload
+                    if (kind[k] == kShared && !(p[k] & claim_bit))
+                        assign_payload<S>(slots + (p[k] & ~claim_bit), S::key(v[k]), found);
+                }
+            }
+            Io<S>::store_payload(out_found, i, found);
+            out_inserted[i] = inserted;
+        }
     }
 }
 
