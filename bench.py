@@ -1036,18 +1036,22 @@ def bloom_part(f_time, g, peak):
     f.Clear()
     ms = time_once(lambda: f.AddAsync(adds))
     res["bloom_add_gkeys"] = round(n / ms / 1e6, 3)
+    # per-key block model: the key plus its 32-byte block read and written
     res["bloom_add_hbm_frac"] = round(n * 72 / (ms / 1e3) / 1e9 / peak, 4)
-    # the same Add through 64-bit atomics (the alternative path); same bits
-    bulk_words = f.words()
-    f.set_add_mode(b2co.BLOOM_ADD_ATOMIC)
-    f.Clear()
-    f.AddAsync(adds)
-    f.Clear()
-    ms = time_once(lambda: f.AddAsync(adds))
-    res["bloom_add_atomic_gkeys"] = round(n / ms / 1e6, 3)
-    res["bloom_add_atomic_equals_bulk"] = bool(np.array_equal(f.words(), bulk_words))
-    del bulk_words
-    f.set_add_mode(b2co.BLOOM_ADD_BULK)
+    # least traffic of any Add: every key read once, the filter read and written once
+    res["bloom_add_hbm_frac_keys_filter"] = round((n * 8 + 2 * nb * 32) / (ms / 1e3) / 1e9 / peak, 4)
+    # the same Add through the other paths; same bits
+    default_words = f.words()
+    for name, mode in (("bulk", b2co.BLOOM_ADD_BULK), ("atomic", b2co.BLOOM_ADD_ATOMIC)):
+        f.set_add_mode(mode)
+        f.Clear()
+        f.AddAsync(adds)
+        f.Clear()
+        ms = time_once(lambda: f.AddAsync(adds))
+        res[f"bloom_add_{name}_gkeys"] = round(n / ms / 1e6, 3)
+        res[f"bloom_add_{name}_equals_default"] = bool(np.array_equal(f.words(), default_words))
+    del default_words
+    f.set_add_mode(b2co.BLOOM_ADD_AUTO)
     out = torch.empty(q.numel(), dtype=torch.uint8, device="cuda")
     f.ContainsAsync(q, out)
     ms = time_once(lambda: f.ContainsAsync(q, out))

@@ -555,10 +555,20 @@ int b2co_bloom_add(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream
 /* How Add of the default policy (8 words per block, one bit per word) updates
  * the filter; the bits set are the same either way.  B2CO_BLOOM_ADD_ATOMIC:
  * four 64-bit atomic ORs per key from the SM.  B2CO_BLOOM_ADD_BULK: one
- * 32-byte TMA bulk reduction (OR) per key from shared memory.  No reference
- * counterpart (the reference chooses between atomics and a routed path by
- * batch size, bloom_filter_launch.inl:131-240).  The default is BULK. */
-typedef enum { B2CO_BLOOM_ADD_ATOMIC = 0, B2CO_BLOOM_ADD_BULK = 1 } b2co_bloom_add_mode;
+ * 32-byte TMA bulk reduction (OR) per key from shared memory.
+ * B2CO_BLOOM_ADD_PARTITIONED: keys are routed by 128 KiB filter slice into a
+ * record workspace (8 bytes per key, at most 2^27 keys per round, allocated on
+ * first use and kept with the filter), then each slice is built in shared
+ * memory and ORed into the filter; filters above 2048 slices (256 MiB) use BULK.
+ * B2CO_BLOOM_ADD_AUTO (the default): PARTITIONED for batches of at least 4 keys
+ * per filter block, BULK otherwise -- the reference likewise chooses between
+ * atomics and a routed path by batch size (bloom_filter_launch.inl:131-240). */
+typedef enum {
+    B2CO_BLOOM_ADD_ATOMIC = 0,
+    B2CO_BLOOM_ADD_BULK = 1,
+    B2CO_BLOOM_ADD_PARTITIONED = 2,
+    B2CO_BLOOM_ADD_AUTO = 3
+} b2co_bloom_add_mode;
 int b2co_bloom_set_add_mode(b2co_bloom* filter, int mode);
 int b2co_bloom_add_async(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream stream);
 int b2co_bloom_add_if(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint64_t n, b2co_stream stream);

@@ -35,7 +35,7 @@ FIND_SEGMENTED = 0x100
 FIND_BULK = 0x200
 FIND_WARP_STAGED = 0x400
 FIND_DEFERRED = 0x800
-BLOOM_ADD_ATOMIC, BLOOM_ADD_BULK = 0, 1
+BLOOM_ADD_ATOMIC, BLOOM_ADD_BULK, BLOOM_ADD_PARTITIONED, BLOOM_ADD_AUTO = 0, 1, 2, 3
 
 
 class B2coError(Exception):
@@ -928,7 +928,10 @@ class BloomFilter:
         return p.value
 
     def set_add_mode(self, mode: int):
-        """BLOOM_ADD_BULK (TMA bulk OR, the default) or BLOOM_ADD_ATOMIC (64-bit atomics) for the default policy's Add."""
+        """How the default policy's Add updates the filter (the bits are the same either way):
+        BLOOM_ADD_ATOMIC (64-bit atomics per key), BLOOM_ADD_BULK (one 32-byte TMA bulk OR per key),
+        BLOOM_ADD_PARTITIONED (keys routed by filter slice, each slice built in shared memory) or
+        BLOOM_ADD_AUTO (the default: partitioned for batches of at least 4 keys per block, else bulk)."""
         _call("b2co_bloom_set_add_mode", self._h, C.c_int(mode))
 
     def words(self) -> np.ndarray:

@@ -125,6 +125,315 @@ __global__ void __launch_bounds__(256) k_bloom_add_bulk(uint32_t* words, uint32_
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // every reduction done before the slots go away
 }
 
+// ---- partitioned Add (default policy, large batches) ------------------------
+// The route-then-apply plan of bloom_filter_launch.inl:131-240 with B200
+// shapes.  The filter is cut into slices of kSliceBlocks blocks (128 KiB); a
+// key's record is its block within the slice (high 32 bits) and the lower
+// hash half (low 32 bits).  Each of R route CTAs owns one contiguous chunk of
+// the batch.
+//   count   : CTA c counts its chunk's records per slice -> counts[c][s];
+//   colscan : per slice, the exclusive prefix over the CTAs (in place) and the
+//             slice's total;
+//   scan    : slice offsets into the record workspace (records of a slice are
+//             contiguous, CTA by CTA);
+//   route   : CTA c hashes its chunk a tile at a time, sorts the tile's
+//             records by slice in shared memory and writes each slice's run at
+//             its own running cursor -- no global atomics, and writes leave in
+//             runs rather than one record at a time;
+//   apply   : one CTA per slice ORs the slice's records into a shared-memory
+//             copy of the slice and reduces the whole copy into the filter with
+//             TMA bulk ORs (element-wise atomic in L2, so concurrent Adds on
+//             other streams stay correct).
+// DRAM traffic per key is the key twice and a record written and read back
+// (8 + 8 + 8 + 8 bytes), against two scattered 32-byte block transfers per key
+// otherwise.
+constexpr uint32_t kSliceBlocks = 4096;
+constexpr uint32_t kMaxSlices = 2048;  // filters up to 256 MiB take this path
+constexpr int kRouteThreads = 1024;
+constexpr int kRouteKeys = 8;  // keys per thread and tile
+constexpr int kRouteTile = kRouteThreads * kRouteKeys;
+constexpr int kApplyThreads = 1024;
+
+// Chunk of route CTA c: whole tiles, the last chunk possibly short.
+__device__ __forceinline__ void route_chunk(uint64_t n, uint32_t c, uint32_t nctas, uint64_t& begin, uint64_t& end)
+{
+    uint64_t const tiles = (n + kRouteTile - 1) / kRouteTile;
+    uint64_t const per = (tiles + nctas - 1) / nctas;
+    begin = uint64_t(c) * per * kRouteTile;
+    end = begin + per * kRouteTile;
+    if (begin > n) begin = n;
+    if (end > n) end = n;
+}
+
+template <int KB>
+__global__ void __launch_bounds__(1024, 2) k_bloom_count(uint32_t nblocks, uint64_t seed, void const* keys,
+                                                     uint8_t const* stencil, uint64_t n, uint32_t nslices,
+                                                     uint32_t nctas, uint32_t* counts)
+{
+    __shared__ uint32_t hist[kMaxSlices];
+    for (uint32_t i = threadIdx.x; i < nslices; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    uint64_t begin, end;
+    route_chunk(n, blockIdx.x, nctas, begin, end);
+    constexpr int kKeys = 8;  // keys loaded before any is hashed
+    for (uint64_t i0 = begin + threadIdx.x; i0 < end; i0 += uint64_t(kKeys) * blockDim.x) {
+        uint64_t key[kKeys];
+        bool live[kKeys];
+#pragma unroll
+        for (int j = 0; j < kKeys; ++j) {
+            uint64_t const i = i0 + uint64_t(j) * blockDim.x;
+            live[j] = i < end && (!stencil || stencil[i]);
+            key[j] = live[j] ? load_key<KB>(keys, i) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < kKeys; ++j) {
+            uint32_t block, lower;
+            locate<KB>(key[j], seed, nblocks, block, lower);
+            if (live[j]) atomicAdd(&hist[block / kSliceBlocks], 1u);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < nslices; i += blockDim.x) counts[uint64_t(blockIdx.x) * nslices + i] = hist[i];
+}
+
+// Per slice (one thread each): exclusive prefix of its counts over the route
+// CTAs, in place, and the slice's total.
+__global__ void __launch_bounds__(256) k_bloom_colscan(uint32_t* counts, uint32_t nslices, uint32_t nctas,
+                                                       uint32_t* totals)
+{
+    uint32_t const sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl >= nslices) return;
+    uint32_t run = 0;
+    for (uint32_t c = 0; c < nctas; ++c) {
+        uint32_t* p = counts + uint64_t(c) * nslices + sl;
+        uint32_t const v = *p;
+        *p = run;
+        run += v;
+    }
+    totals[sl] = run;
+}
+
+// Exclusive scan of the slice totals (one CTA): offsets[0..nslices].
+__global__ void __launch_bounds__(1024) k_bloom_scan(uint32_t const* totals, uint32_t nslices, uint32_t* offsets)
+{
+    __shared__ uint32_t warp_tot[32];
+    constexpr int kPer = kMaxSlices / 1024;
+    uint32_t const t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    uint32_t v[kPer], sum = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        uint32_t const i = t * kPer + j;
+        v[j] = i < nslices ? totals[i] : 0u;
+        sum += v[j];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= uint32_t(d)) incl += o;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t const w = warp_tot[lane];
+        uint32_t wi = w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t const o = __shfl_up_sync(0xffffffffu, wi, d);
+            if (lane >= uint32_t(d)) wi += o;
+        }
+        warp_tot[lane] = wi - w;  // exclusive prefix of the warp totals
+    }
+    __syncthreads();
+    uint32_t run = warp_tot[warp] + incl - sum;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        uint32_t const i = t * kPer + j;
+        if (i <= nslices) offsets[i] = run;
+        run += v[j];
+    }
+    if (t == 1023 && nslices == kMaxSlices) offsets[nslices] = run;
+}
+
+// Shared memory of one route CTA: the tile's records and their destinations,
+// then per slice the tile's count, its offset in the tile, its run's global
+// start, the CTA's running cursor and the slice's end in the workspace.
+constexpr size_t kRouteSmem = size_t(kRouteTile) * (8 + 4) + size_t(kMaxSlices) * 4 * 5 + (kRouteThreads / 32 + 1) * 4;
+
+template <int KB>
+__global__ void __launch_bounds__(kRouteThreads) k_bloom_route(uint32_t nblocks, uint64_t seed, void const* keys,
+                                                               uint8_t const* stencil, uint64_t n, uint32_t nslices,
+                                                               uint32_t nctas, uint32_t const* prefix,
+                                                               uint32_t const* offsets, unsigned long long* recs)
+{
+    extern __shared__ __align__(16) unsigned char route_smem[];
+    auto* stage = reinterpret_cast<unsigned long long*>(route_smem);
+    auto* stage_at = reinterpret_cast<uint32_t*>(stage + kRouteTile);
+    uint32_t* hist = stage_at + kRouteTile;
+    uint32_t* loff = hist + kMaxSlices;
+    uint32_t* gbase = loff + kMaxSlices;
+    uint32_t* gcur = gbase + kMaxSlices;
+    uint32_t* gend = gcur + kMaxSlices;
+    uint32_t* warp_tot = gend + kMaxSlices;  // kRouteThreads / 32 warp sums, then the tile's total
+    uint32_t const t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    constexpr uint32_t kNone = 0xffffffffu;
+    constexpr int kWarps = kRouteThreads / 32;
+    constexpr int kPer = kMaxSlices / kRouteThreads;
+    for (uint32_t i = t; i < nslices; i += kRouteThreads) {
+        gcur[i] = offsets[i] + prefix[uint64_t(blockIdx.x) * nslices + i];
+        gend[i] = offsets[i + 1];
+    }
+    uint64_t begin, end;
+    route_chunk(n, blockIdx.x, nctas, begin, end);
+    for (uint64_t base = begin; base < end; base += kRouteTile) {
+        for (uint32_t i = t; i < nslices; i += kRouteThreads) hist[i] = 0;
+        __syncthreads();
+        // every key of the thread is loaded before any shared-memory atomic, so
+        // the loads are in flight together; a record's rank within its slice
+        // comes from the shared histogram
+        unsigned long long rec[kRouteKeys];
+        uint32_t where[kRouteKeys];  // slice << 16 | rank in the tile, or kNone
+        uint64_t key[kRouteKeys];
+        bool live[kRouteKeys];
+#pragma unroll
+        for (int j = 0; j < kRouteKeys; ++j) {
+            uint64_t const i = base + uint64_t(j) * kRouteThreads + t;
+            live[j] = i < end && (!stencil || stencil[i]);
+            key[j] = live[j] ? load_key<KB>(keys, i) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < kRouteKeys; ++j) {
+            uint32_t block, lower;
+            locate<KB>(key[j], seed, nblocks, block, lower);
+            rec[j] = (uint64_t(block % kSliceBlocks) << 32) | lower;
+            where[j] = block / kSliceBlocks;
+        }
+#pragma unroll
+        for (int j = 0; j < kRouteKeys; ++j)
+            where[j] = live[j] ? (where[j] << 16) | atomicAdd(&hist[where[j]], 1u) : kNone;
+        __syncthreads();
+        // the tile's offsets per slice (exclusive scan, kPer slices per thread);
+        // each slice's run starts at the CTA's cursor for it
+        uint32_t v[kPer], sum = 0;
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            uint32_t const i = t * kPer + q;
+            v[q] = i < nslices ? hist[i] : 0u;
+            sum += v[q];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t const o = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= uint32_t(d)) incl += o;
+        }
+        if (lane == 31) warp_tot[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t const w = lane < kWarps ? warp_tot[lane] : 0u;
+            uint32_t wi = w;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                uint32_t const o = __shfl_up_sync(0xffffffffu, wi, d);
+                if (lane >= uint32_t(d)) wi += o;
+            }
+            if (lane < kWarps) warp_tot[lane] = wi - w;
+            if (lane == 31) warp_tot[kWarps] = wi;  // the tile's record count
+        }
+        __syncthreads();
+        uint32_t run = warp_tot[warp] + incl - sum;
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            uint32_t const i = t * kPer + q;
+            if (i < nslices) {
+                loff[i] = run;
+                gbase[i] = gcur[i];
+                gcur[i] += v[q];
+            }
+            run += v[q];
+        }
+        __syncthreads();
+        // records sorted by slice in shared memory, each with its destination; a
+        // record never passes its slice's end (only keys changed between the
+        // count and this pass could ask it to)
+#pragma unroll
+        for (int j = 0; j < kRouteKeys; ++j) {
+            if (where[j] == kNone) continue;
+            uint32_t const sl = where[j] >> 16, r = where[j] & 0xffffu, g = gbase[sl] + r;
+            stage[loff[sl] + r] = rec[j];
+            stage_at[loff[sl] + r] = g < gend[sl] ? g : kNone;
+        }
+        __syncthreads();
+        // each slice's records leave as one run
+        uint32_t const total = warp_tot[kWarps];
+        for (uint32_t at = t; at < total; at += kRouteThreads) {
+            uint32_t const g = stage_at[at];
+            if (g != kNone) recs[g] = stage[at];
+        }
+        // the next tile rewrites the shared arrays only after its first barrier
+    }
+}
+
+// One CTA per slice: OR the slice's records into a shared copy of its words,
+// then bulk-OR the copy into the filter in 16 KiB pieces.
+constexpr uint32_t kApplyChunk = 16384;
+
+__global__ void __launch_bounds__(kApplyThreads) k_bloom_apply(uint32_t* words, uint32_t nblocks,
+                                                               unsigned long long const* recs,
+                                                               uint32_t const* offsets)
+{
+    extern __shared__ __align__(128) uint32_t slice[];  // kSliceBlocks * 8 words
+    uint32_t const sl = blockIdx.x, first = sl * kSliceBlocks;
+    uint32_t const nb = nblocks - first < kSliceBlocks ? nblocks - first : kSliceBlocks;
+    uint32_t const nwords = nb * 8;
+    for (uint32_t i = threadIdx.x * 4; i < nwords; i += kApplyThreads * 4)
+        *reinterpret_cast<uint4*>(slice + i) = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    uint32_t const beg = offsets[sl], end = offsets[sl + 1];
+    for (uint32_t r = beg + threadIdx.x; r < end; r += kApplyThreads) {
+        unsigned long long const rec = __ldcs(recs + r);
+        uint32_t const b = uint32_t(rec >> 32), lower = uint32_t(rec);
+        if (b >= nb) continue;
+        // word w of block b sits at b * 8 + (w ^ swz(b)): the words that a warp
+        // writes in one step spread over the banks instead of four of them
+        uint32_t* blk = slice + b * 8;
+        uint32_t const swz = (b >> 2) & 7u;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) atomicOr(blk + (uint32_t(w) ^ swz), word_bit(w, lower));
+    }
+    __syncthreads();
+    // back to the filter's word order, a block per thread
+    for (uint32_t b = threadIdx.x; b < nb; b += kApplyThreads) {
+        uint32_t* blk = slice + b * 8;
+        uint32_t const swz = (b >> 2) & 7u;
+        uint4 const lo = *reinterpret_cast<uint4 const*>(blk), hi = *reinterpret_cast<uint4 const*>(blk + 4);
+        uint32_t const x[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+        uint32_t y[8];
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            uint32_t v = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v = (uint32_t(j) == (uint32_t(w) ^ swz)) ? x[j] : v;
+            y[w] = v;
+        }
+        *reinterpret_cast<uint4*>(blk) = make_uint4(y[0], y[1], y[2], y[3]);
+        *reinterpret_cast<uint4*>(blk + 4) = make_uint4(y[4], y[5], y[6], y[7]);
+    }
+    fence_proxy_async();  // this thread's shared-memory writes precede the bulk reads
+    __syncthreads();
+    uint32_t const bytes = nwords * 4;
+    if (threadIdx.x < (bytes + kApplyChunk - 1) / kApplyChunk) {
+        uint32_t const off = threadIdx.x * kApplyChunk;
+        uint32_t const len = bytes - off < kApplyChunk ? bytes - off : kApplyChunk;
+        asm volatile("cp.reduce.async.bulk.global.shared::cta.bulk_group.or.b32 [%0], [%1], %2;" ::"l"(
+                         words + uint64_t(first) * 8 + off / 4),
+                     "r"(smem_u32(slice) + off), "r"(len)
+                     : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    }
+}
+
 template <int KB>
 __global__ void __launch_bounds__(256) k_bloom_contains(uint32_t const* words, uint32_t nblocks, uint64_t seed,
                                                         void const* keys, uint8_t const* stencil, uint8_t* out,
@@ -251,7 +560,11 @@ cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 
 struct b2co_bloom {
     uint32_t* words = nullptr;
-    int add_mode = B2CO_BLOOM_ADD_BULK;  // default-policy Add: bulk reductions (measured faster) or 64-bit atomics
+    int add_mode = B2CO_BLOOM_ADD_AUTO;  // default-policy Add: see b2co_bloom_add_mode
+    unsigned long long* recs = nullptr;  // partitioned Add: record workspace
+    uint64_t recs_cap = 0;
+    uint32_t* part = nullptr;  // partitioned Add: per-CTA slice counts, slice totals and offsets
+    size_t part_words = 0;
     uint64_t num_blocks = 0;
     uint32_t key_bytes = 0;
     uint64_t seed = 0;
@@ -319,6 +632,64 @@ int launch_contains_policy(b2co_bloom* f, void const* keys, uint8_t const* stenc
     return B2CO_OK;
 }
 
+// Batches of at least this many keys per filter block take the partitioned
+// Add under B2CO_BLOOM_ADD_AUTO: below it, writing the whole filter back once
+// per launch outweighs what routing saves.
+constexpr uint64_t kPartitionKeysPerBlock = 4;
+// Keys per route-and-apply round (the record workspace holds this many).
+constexpr uint64_t kPartitionRound = uint64_t(1) << 27;
+
+template <int KB>
+int launch_add_partitioned(b2co_bloom* f, void const* keys, uint8_t const* stencil, uint64_t n, cudaStream_t s)
+{
+    uint32_t const nblocks = uint32_t(f->num_blocks);
+    uint32_t const nslices = (nblocks + kSliceBlocks - 1) / kSliceBlocks;
+    uint64_t const want = n < kPartitionRound ? n : kPartitionRound;
+    if (f->recs_cap < want) {
+        if (f->recs) cudaFree(f->recs);
+        f->recs = nullptr;
+        f->recs_cap = 0;
+        B2CO_CUDA(cudaMalloc(&f->recs, want * 8));
+        f->recs_cap = want;
+    }
+    auto const route = k_bloom_route<KB>;
+    auto const count = k_bloom_count<KB>;
+    size_t const apply_smem = size_t(kSliceBlocks) * 32;
+    B2CO_CUDA(cudaFuncSetAttribute((void const*)route, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kRouteSmem)));
+    B2CO_CUDA(cudaFuncSetAttribute((void const*)k_bloom_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(apply_smem)));
+    int per_sm = 0;
+    B2CO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)route, kRouteThreads, kRouteSmem));
+    uint32_t const route_cap = uint32_t(per_sm < 1 ? 1 : per_sm) * uint32_t(sm_count());
+    // counts[route CTA][slice], then the slice totals and offsets
+    size_t const part_words = size_t(route_cap) * kMaxSlices + 2 * size_t(kMaxSlices) + 1;
+    if (f->part_words < part_words) {
+        if (f->part) cudaFree(f->part);
+        f->part = nullptr;
+        f->part_words = 0;
+        B2CO_CUDA(cudaMalloc(&f->part, part_words * 4));
+        f->part_words = part_words;
+    }
+    uint32_t* counts = f->part;
+    uint32_t* totals = counts + size_t(route_cap) * kMaxSlices;
+    uint32_t* offsets = totals + kMaxSlices;
+    for (uint64_t at = 0; at < n; at += kPartitionRound) {
+        uint64_t const m = n - at < kPartitionRound ? n - at : kPartitionRound;
+        void const* k = static_cast<char const*>(keys) + at * KB;
+        uint8_t const* st = stencil ? stencil + at : nullptr;
+        uint64_t const tiles = (m + kRouteTile - 1) / kRouteTile;
+        uint32_t const nctas = uint32_t(tiles < route_cap ? tiles : route_cap);
+        count<<<nctas, 1024, 0, s>>>(nblocks, f->seed, k, st, m, nslices, nctas, counts);
+        k_bloom_colscan<<<(nslices + 255) / 256, 256, 0, s>>>(counts, nslices, nctas, totals);
+        k_bloom_scan<<<1, 1024, 0, s>>>(totals, nslices, offsets);
+        route<<<nctas, kRouteThreads, kRouteSmem, s>>>(nblocks, f->seed, k, st, m, nslices, nctas, counts, offsets,
+                                                      f->recs);
+        k_bloom_apply<<<nslices, kApplyThreads, apply_smem, s>>>(f->words, nblocks, f->recs, offsets);
+    }
+    B2CO_CUDA(cudaGetLastError());
+    return B2CO_OK;
+}
+
 int add_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_stencil, uint64_t n, cudaStream_t s)
 {
     if (int st = check(f)) return st;
@@ -328,8 +699,15 @@ int add_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_s
         return fail(B2CO_EINVAL, "BloomFilter::AddIf: stencil must not be null when keyNum is non-zero");
     if (!f->default_policy())
         return f->key_bytes == 8 ? launch_add_policy<8>(f, keys, stencil, n, s) : launch_add_policy<4>(f, keys, stencil, n, s);
+    uint64_t const nslices = (f->num_blocks + kSliceBlocks - 1) / kSliceBlocks;
+    bool const part = nslices <= kMaxSlices &&
+                      (f->add_mode == B2CO_BLOOM_ADD_PARTITIONED ||
+                       (f->add_mode == B2CO_BLOOM_ADD_AUTO && n >= kPartitionKeysPerBlock * f->num_blocks));
+    if (part)
+        return f->key_bytes == 8 ? launch_add_partitioned<8>(f, keys, stencil, n, s)
+                                 : launch_add_partitioned<4>(f, keys, stencil, n, s);
     void (*k)(uint32_t*, uint32_t, uint64_t, void const*, uint8_t const*, uint64_t) = nullptr;
-    if (f->add_mode == B2CO_BLOOM_ADD_BULK) k = f->key_bytes == 8 ? k_bloom_add_bulk<8> : k_bloom_add_bulk<4>;
+    if (f->add_mode != B2CO_BLOOM_ADD_ATOMIC) k = f->key_bytes == 8 ? k_bloom_add_bulk<8> : k_bloom_add_bulk<4>;
     else k = f->key_bytes == 8 ? k_bloom_add<8> : k_bloom_add<4>;
     k<<<grid_for((void const*)k, 256, n, 256), 256, 0, s>>>(f->words, uint32_t(f->num_blocks), f->seed, keys, stencil,
                                                            n);
@@ -431,6 +809,8 @@ int b2co_bloom_destroy(b2co_bloom* f)
 {
     if (!f) return B2CO_OK;
     if (f->words) cudaFree(f->words);
+    if (f->recs) cudaFree(f->recs);
+    if (f->part) cudaFree(f->part);
     delete f;
     return B2CO_OK;
 }
@@ -545,7 +925,7 @@ extern "C" {
 int b2co_bloom_set_add_mode(b2co_bloom* f, int mode)
 {
     if (int st = check(f)) return st;
-    if (mode != B2CO_BLOOM_ADD_ATOMIC && mode != B2CO_BLOOM_ADD_BULK) return fail(B2CO_EINVAL, "unknown Add mode");
+    if (mode < B2CO_BLOOM_ADD_ATOMIC || mode > B2CO_BLOOM_ADD_AUTO) return fail(B2CO_EINVAL, "unknown Add mode");
     f->add_mode = mode;
     return B2CO_OK;
 }

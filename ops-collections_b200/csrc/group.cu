@@ -450,8 +450,7 @@ int b2co_oa_group_autotune(b2co_oa_group* g, void const* keys, uint64_t const* d
         int st = B2CO_OK;
         for (uint32_t ln : kLanes) {
             for (uint32_t it : kItems) {
-                // one lane takes 2 or 4 keys in flight only with buckets of 5
-                if ((ln == 1 && it > 1 && g->desc.bucket_size != 5) || (ln > 1 && it > ln)) continue;
+                if ((ln == 1 && it > 1) || (ln > 1 && it > ln)) continue;
                 for (uint32_t bl : kBlocks) {
                     g->find_shape = ln | (it << 8) | (bl << 16);
                     if ((st = b2co_oa_group_find(g, keys, d_offsets, out, n, 0, s))) break;  // warm

@@ -64,66 +64,49 @@ __device__ __forceinline__ void warp_span(uint64_t n, uint32_t step, uint64_t& b
 }
 
 // One lane per key: the window is scanned in the lane's own registers, with no
-// ballots or shuffles, and a key that needs further windows walks on alone.  A
-// lane loads the first windows of K keys (items lane, lane + 32, ...) before it
-// scans any of them.
-template <class S, int B, bool CONTAINS, int K>
+// ballots or shuffles, and a key that needs further windows walks on alone.
+template <class S, int B, bool CONTAINS>
 __device__ __forceinline__ void group_find_lane(GroupArgs const& g, void const* keys, void* out, uint64_t begin,
                                                 uint64_t end)
 {
     using Raw = typename S::Raw;
     uint32_t const lane = threadIdx.x & 31;
     uint32_t t = group_table_of(g.offsets, g.count, begin + lane < end ? begin + lane : begin);
+    OaArgs a = group_table_args<S>(g, t);
     uint64_t next_off = __ldg(g.offsets + t + 1);
-    OaArgs cur = group_table_args<S>(g, t);
-    for (uint64_t i0 = begin + lane; i0 < end; i0 += 32u * K) {
-        uint64_t key[K];
-        uint32_t init[K];
-        OaArgs a[K];
-        Raw w[K][B];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            uint64_t const i = i0 + 32u * k;
-            if (i >= end) continue;
-            if (i >= next_off) {
-                do next_off = __ldg(g.offsets + ++t + 1);
-                while (i >= next_off);
-                cur = group_table_args<S>(g, t);
-            }
-            a[k] = cur;
-            key[k] = uint64_t(__ldg(reinterpret_cast<typename Io<S>::Key const*>(keys) + i));
-            init[k] = probe_init<S::key_bytes, B>(cur.probe, key[k]);
-            load_window<S, B>(reinterpret_cast<Raw const*>(cur.slots), init[k], w[k]);
+    for (uint64_t i = begin + lane; i < end; i += 32) {
+        if (i >= next_off) {
+            do {
+                ++t;
+                next_off = __ldg(g.offsets + t + 1);
+            } while (i >= next_off);
+            a = group_table_args<S>(g, t);
         }
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            uint64_t const i = i0 + 32u * k;
-            if (i >= end) continue;
-            OaArgs const& at = a[k];
-            Raw stop;
-            uint64_t payload = empty_payload<S>(at);
-            bool hit;
-            if (scan_window<S, B>(w[k], key[k], at.empty_key, stop)) {
-                hit = S::key(stop) != at.empty_key;
-                if (hit) payload = S::value(stop);
-            } else {
-                hit = find_rest<S, B>(at, key[k], init[k], payload);
-            }
-            if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = hit;
-            else reinterpret_cast<typename Io<S>::Payload*>(out)[i] =
-                typename Io<S>::Payload(hit ? payload : empty_payload<S>(at));
+        uint64_t const key = uint64_t(__ldg(reinterpret_cast<typename Io<S>::Key const*>(keys) + i));
+        uint32_t const init = probe_init<S::key_bytes, B>(a.probe, key);
+        Raw w[B];
+        load_window<S, B>(reinterpret_cast<Raw const*>(a.slots), init, w);
+        Raw stop;
+        uint64_t payload = empty_payload<S>(a);
+        bool hit;
+        if (scan_window<S, B>(w, key, a.empty_key, stop)) {
+            hit = S::key(stop) != a.empty_key;
+            if (hit) payload = S::value(stop);
+        } else {
+            hit = find_rest<S, B>(a, key, init, payload);
         }
+        if constexpr (CONTAINS) reinterpret_cast<uint8_t*>(out)[i] = hit;
+        else reinterpret_cast<typename Io<S>::Payload*>(out)[i] = typename Io<S>::Payload(hit ? payload : empty_payload<S>(a));
     }
 }
 
-// K: keys in flight per lane with one lane per key (G = 1).
-template <class S, int B, int G, bool CONTAINS, int K = 1>
+template <class S, int B, int G, bool CONTAINS>
 __global__ void __launch_bounds__(256) k_group_find(GroupArgs g, void const* keys, void* out, uint64_t n)
 {
     if constexpr (G == 1) {
         uint64_t begin, end;
         warp_span(n, 32, begin, end);
-        if (begin < end) group_find_lane<S, B, CONTAINS, K>(g, keys, out, begin, end);
+        if (begin < end) group_find_lane<S, B, CONTAINS>(g, keys, out, begin, end);
         return;
     }
     using Raw = typename S::Raw;

@@ -375,10 +375,8 @@ struct GroupImpl {
 
     // `shape` packs lanes per window (bits 0-7), keys in flight per lane group
     // (bits 8-15; 1 = one key per tile, resolved at once) and threads per block
-    // (bits 16-31; 0 = 256).  With 2 or more lanes, keys per tile above 1 run
-    // the deferred kernel; its 2-, 4- and 8-lane variants other than 4x2 exist
-    // for bucket size 5.  With one lane, 2 or 4 keys per tile are the keys a
-    // lane loads before it scans (bucket size 5; otherwise 1).
+    // (bits 16-31; 0 = 256).  Keys per tile above 1 run the deferred kernel;
+    // its 2-, 4- and 8-lane variants other than 4x2 exist for bucket size 5.
     template <int B, bool C>
     static int find_b(GroupArgs const& g, uint32_t shape, void const* keys, void* out, uint64_t n, cudaStream_t s)
     {
@@ -394,10 +392,6 @@ struct GroupImpl {
             if (!k) k = k_group_find_q<S, B, 4, 2, C>;
         } else if (lanes <= 1) {
             k = k_group_find<S, B, 1, C>;
-            if constexpr (B == 5) {
-                if (items == 2) k = k_group_find<S, B, 1, C, 2>;
-                else if (items >= 4) k = k_group_find<S, B, 1, C, 4>;
-            }
         } else if (lanes == 2) {
             k = k_group_find<S, B, 2, C>;
         } else if (lanes == 4) {

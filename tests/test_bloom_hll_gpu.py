@@ -12,12 +12,13 @@ from helpers import dev
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("mode", ["atomic", "bulk"])
+@pytest.mark.parametrize("mode", ["atomic", "bulk", "partitioned", "auto"])
 @pytest.mark.parametrize("kdt", [np.uint32, np.int32, np.uint64, np.int64, np.float32])
-@pytest.mark.parametrize("num_blocks", [1, 7, 4096, 1 << 16])
+@pytest.mark.parametrize("num_blocks", [1, 7, 4096, 5000, 1 << 16])
 def test_bloom_add_contains_bit_exact(kdt, num_blocks, mode):
-    """Both Add paths of the default policy (64-bit atomics, TMA bulk ORs) set
-    exactly the oracle's bits."""
+    """Every Add path of the default policy (64-bit atomics, TMA bulk ORs, keys
+    routed by filter slice, and the automatic choice) sets exactly the oracle's
+    bits; 4096 blocks is one whole slice, 5000 ends in a partial one."""
     import b2co
     import torch
     rng = np.random.default_rng(int(num_blocks) + np.dtype(kdt).itemsize)
@@ -30,7 +31,8 @@ def test_bloom_add_contains_bit_exact(kdt, num_blocks, mode):
     ktorch = {np.uint32: torch.int32, np.int32: torch.int32, np.float32: torch.int32,
               np.uint64: torch.int64, np.int64: torch.int64}[kdt]
     f = b2co.BloomFilter(num_blocks, key_dtype=ktorch)
-    f.set_add_mode(b2co.BLOOM_ADD_BULK if mode == "bulk" else b2co.BLOOM_ADD_ATOMIC)
+    f.set_add_mode({"atomic": b2co.BLOOM_ADD_ATOMIC, "bulk": b2co.BLOOM_ADD_BULK,
+                    "partitioned": b2co.BLOOM_ADD_PARTITIONED, "auto": b2co.BLOOM_ADD_AUTO}[mode])
     kd = torch.from_numpy(keys.view(np.int32 if keys.itemsize == 4 else np.int64)).cuda()
     f.Add(kd[: n // 2])
     f.AddAsync(kd[n // 2:])
@@ -160,8 +162,8 @@ def test_hll_registers_bit_exact(precision, key_bytes):
     h = b2co.HyperLogLog(precision, key_dtype=torch.int32 if key_bytes == 4 else torch.int64)
     kd = dev(keys)
     h.Add(kd[:100])          # tiny batch
-    h.Add(kd[100:300000])    # medium
-    h.Add(kd[300000:])       # large
+    h.Add(kd[100:300001])    # medium, ragged end
+    h.Add(kd[300001:])       # large, starts off a 16-byte boundary
     reg = np.zeros(1 << precision, np.uint8)
     oracle.hll_add(reg, precision, keys)
     assert np.array_equal(h.registers(), reg)
