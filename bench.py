@@ -457,10 +457,11 @@ def pcie_floor_ms(hq, ho, q, out):
 
 def window_gather_ceiling(t, stream, find_gkeys, windows_mean):
     """The random bucket-window read rate of this GPU over the very same table:
-    bare reads of whole 80-byte windows at random bucket starts, none of a
-    lookup's other work (key stream, hashing, outputs, second windows).  Random
-    80-byte windows move whole DRAM fill units, so this rate, not the copy peak,
-    is what Find can approach; timed after (never inside) the Find region."""
+    bare reads of whole windows (80 bytes for 16-byte slots, 40 for 8-byte) at
+    random bucket starts, none of a lookup's other work (key stream, hashing,
+    outputs, second windows).  Random windows move whole DRAM fill units, so
+    this rate, not the copy peak, is what Find can approach; timed after (never
+    inside) the Find region."""
     import torch
     n = 1 << 27
     for i in range(3):
@@ -954,6 +955,15 @@ def batched_measurements(stream):
     del graph
     res["batched_per_table_equals_group"] = bool(torch.equal(out2, ref))
     res["batched_hits_found"] = bool(((ref != -1) == hit).all().item())
+    del out2, per
+    # the random-window ceiling for these 8-byte slots: bare 40-byte window reads
+    # over one table with as many slots as the whole group (after the timed regions)
+    flat = b2co.StaticMap(grp.total_slots(), -1, -1, key_dtype=torch.int32, value_dtype=torch.int32)
+    ceil = window_gather_ceiling(flat, stream, res["batched_group_find_gkeys"], None)
+    res["batched_window_gather_ceiling_gwin"] = ceil["window_gather_ceiling_gwin"]
+    # every query reads at least one window, so this is a lower bound of the share of the ceiling used
+    res["batched_find_queries_vs_ceiling"] = round(res["batched_group_find_gkeys"] / ceil["window_gather_ceiling_gwin"], 4)
+    del flat
     return res
 
 

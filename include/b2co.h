@@ -137,7 +137,7 @@ int b2co_oa_data(const b2co_oa_table* table, void** slots);
 int b2co_oa_describe(const b2co_oa_table* table, b2co_oa_desc* desc);
 /* Measurement aid (no reference counterpart): `n` (<= 2^31) reads of whole
  * bucket windows at pseudo-random bucket starts (`seed`) of the table's own
- * slots, four lanes per window, nothing written.  16-byte slots only.  Timing it
+ * slots, four lanes per window, nothing written.  16- or 8-byte slots.  Timing it
  * gives the random-window read rate a lookup's first windows can reach on this
  * GPU, the practical ceiling of Find beside the HBM copy peak. */
 int b2co_oa_window_gather(const b2co_oa_table* table, uint64_t n, uint32_t seed, b2co_stream stream);
@@ -189,10 +189,9 @@ int b2co_oa_reserve_insert_and_find(b2co_oa_table* table, uint64_t n);
  * per table slot) comes from a fixed 32 MiB device array inside the library,
  * which every GPU that loads the library holds until the process exits.
  * Batches needing more scratch fail with B2CO_ERANGE.  Every call looks up
- * the array's address on the current device; the first call on a device also
- * loads the array there, so make that call before any stream capture begins.
- * All calls share the array, so calls that overlap on the GPU race: serialize
- * them. */
+ * the array's address on the current device.  The call ends by synchronizing
+ * its stream, so it cannot be captured into a CUDA graph.  All calls share the
+ * array, so calls that overlap on the GPU race: serialize them. */
 int b2co_oa_insert_and_find_noalloc(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
                                     uint64_t n, b2co_stream stream);
 /* Erase (returns the count of keys not erased).

@@ -340,7 +340,7 @@ class _OaBase:
               C.c_uint64(n), _stream(stream))
 
     def window_gather(self, n: int, seed: int = 0, stream=None):
-        """Bare random bucket-window reads over this table's slots (16-byte slots; a measurement aid)."""
+        """Bare random bucket-window reads over this table's slots (16- or 8-byte slots; a measurement aid)."""
         _call("b2co_oa_window_gather", self._h, C.c_uint64(n), C.c_uint32(seed), _stream(stream))
 
     def set_find_shape(self, lanes_per_key: int, keys_per_lane: int, segmented: bool = False, bulk: bool = False,

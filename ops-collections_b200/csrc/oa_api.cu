@@ -284,13 +284,17 @@ __device__ __forceinline__ uint32_t gather_mix(uint32_t x)
     return x;
 }
 
-// Bare random bucket-window reads over a table's own 16-byte slots: the rate the
-// first-window reads of a lookup can reach on this GPU, with none of a lookup's
-// other work.  Four lanes per window and four windows in flight per lane group
-// (the fastest form measured); bucket b = mix(i ^ seed) % nbuckets, so every read
-// stays inside the slot array.  Nothing is written but a sink word no real sum meets.
-template <int B>
-__global__ void __launch_bounds__(256) k_window_gather(U128 const* slots, uint32_t nbuckets, uint32_t n, uint32_t seed)
+// Bare random bucket-window reads over a table's own 16- or 8-byte slots: the
+// rate the first-window reads of a lookup can reach on this GPU, with none of a
+// lookup's other work.  Four lanes per window and four windows in flight per lane
+// group (the fastest form measured); bucket b = mix(i ^ seed) % nbuckets, so every
+// read stays inside the slot array.  Nothing is written but a sink word no real
+// sum meets.
+__device__ __forceinline__ unsigned long long fold_slot(U128 v) { return v.lo + v.hi; }
+__device__ __forceinline__ unsigned long long fold_slot(unsigned long long v) { return v; }
+
+template <int B, class W>
+__global__ void __launch_bounds__(256) k_window_gather(W const* slots, uint32_t nbuckets, uint32_t n, uint32_t seed)
 {
     constexpr int G = 4, K = 4, R = (B + G - 1) / G;
     uint32_t const r = threadIdx.x % G;
@@ -298,7 +302,7 @@ __global__ void __launch_bounds__(256) k_window_gather(U128 const* slots, uint32
     uint32_t const g0 = blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
     unsigned long long acc = 0;
     for (uint32_t base = g0; base < n; base += groups * K) {
-        U128 w[K][R];
+        W w[K][R];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             uint32_t const i = base + k * groups;
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(256) k_window_gather(U128 const* slots, uint32
         for (int k = 0; k < K; ++k)
 #pragma unroll
             for (int s = 0; s < R; ++s)
-                if (base + k * groups < n && int(r) + s * G < B) acc ^= w[k][s].lo + w[k][s].hi;
+                if (base + k * groups < n && int(r) + s * G < B) acc ^= fold_slot(w[k][s]);
     }
     if (acc == 0x9e3779b97f4a7c15ull) g_gather_sink = acc;  // keeps the reads live
 }
@@ -323,25 +327,32 @@ extern "C" {
 int b2co_oa_window_gather(b2co_oa_table const* t, uint64_t n, uint32_t seed, b2co_stream stream)
 {
     if (int st = check_table(t)) return st;
-    if (slot_bytes(t->desc.key_bytes, t->desc.value_bytes) != 16)
-        return fail(B2CO_EINVAL, "window gather needs 16-byte slots");
+    uint32_t const sb = slot_bytes(t->desc.key_bytes, t->desc.value_bytes);
+    if (sb != 16 && sb != 8) return fail(B2CO_EINVAL, "window gather needs 16- or 8-byte slots");
     if (n > (1ull << 31)) return fail(B2CO_ERANGE, "window gather: at most 2^31 windows per call");
     if (n == 0) return B2CO_OK;
     uint32_t const b = t->desc.bucket_size;
     uint32_t const nb = uint32_t(t->capacity / b);
-    U128 const* slots = static_cast<U128 const*>(t->args.slots);
-    void (*k)(U128 const*, uint32_t, uint32_t, uint32_t) = nullptr;
-    switch (b) {
-    case 1: k = k_window_gather<1>; break;
-    case 2: k = k_window_gather<2>; break;
-    case 4: k = k_window_gather<4>; break;
-    case 5: k = k_window_gather<5>; break;
-    case 8: k = k_window_gather<8>; break;
-    default: return fail(B2CO_EINVAL, "unsupported bucket size");
-    }
-    uint32_t grid = grid_for((void const*)k, 256, n, 64);
-    k<<<grid, 256, 0, cs(stream)>>>(slots, nb, uint32_t(n), seed);
-    cudaError_t e = cudaGetLastError();
+    void const* k = nullptr;
+    auto pick = [&](auto w) {
+        using W = decltype(w);
+        switch (b) {
+        case 1: k = (void const*)k_window_gather<1, W>; break;
+        case 2: k = (void const*)k_window_gather<2, W>; break;
+        case 4: k = (void const*)k_window_gather<4, W>; break;
+        case 5: k = (void const*)k_window_gather<5, W>; break;
+        case 8: k = (void const*)k_window_gather<8, W>; break;
+        default: break;
+        }
+    };
+    if (sb == 16) pick(U128{});
+    else pick(0ull);
+    if (!k) return fail(B2CO_EINVAL, "unsupported bucket size");
+    uint32_t grid = grid_for(k, 256, n, 64);
+    void const* slots = t->args.slots;
+    uint32_t n32 = uint32_t(n);
+    void* params[] = {(void*)&slots, (void*)&nb, (void*)&n32, (void*)&seed};
+    cudaError_t e = cudaLaunchKernel(k, dim3(grid), dim3(256), params, 0, cs(stream));
     return e == cudaSuccess ? B2CO_OK : cuda_fail(e, "window gather kernel");
 }
 

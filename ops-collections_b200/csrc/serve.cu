@@ -67,7 +67,16 @@ struct Request {
     uint64_t in_bytes = 0, out_bytes = 0;
     bool taken = false;  // admitted (possibly ahead of the queue's head); popped lazily
     std::atomic<bool> done{false};
+    // Two owners: the dispatcher's queue (until it pops the request, which may be
+    // long after the request finished, since requests are admitted out of
+    // order) and the caller (until its wait returns).  The last one frees it.
+    std::atomic<int> refs{2};
 };
+
+void unref(Request* r)
+{
+    if (r->refs.fetch_sub(1, std::memory_order_acq_rel) == 1) delete r;
+}
 
 bool is_write(Request const* r) { return r->info.op == B2CO_OP_INSERT || r->info.op == B2CO_OP_INSERT_OR_ASSIGN; }
 
@@ -473,6 +482,16 @@ struct b2co_server {
         cv_done.notify_all();
     }
 
+    // Drops the admitted requests at the queue's head (the queue's reference).
+    void pop_taken()
+    {
+        while (!queue.empty() && queue.front()->taken) {
+            Request* r = queue.front();
+            queue.pop_front();
+            unref(r);
+        }
+    }
+
     // Plain mode's admission: the earliest arrived request of each table that
     // has no launch in flight, alone, in arrival order per table (tables run
     // side by side on the slots).
@@ -480,7 +499,7 @@ struct b2co_server {
     {
         bool progress = false;
         uint64_t const t = now_ns();
-        while (!queue.empty() && queue.front()->taken) queue.pop_front();
+        pop_taken();
         std::vector<b2co_oa_table const*> blocked;
         for (auto& sl : slots)
             if (sl.busy) blocked.push_back(sl.reqs.front()->table);
@@ -526,7 +545,7 @@ struct b2co_server {
         bool progress = false;
         uint64_t const t = now_ns();
         for (;;) {
-            while (!queue.empty() && queue.front()->taken) queue.pop_front();
+            pop_taken();
             if (queue.empty() || queue.front()->info.arrival_ns > t) return progress;
             std::vector<Request*> g = group_at_head(t);
             Slot* sl = pick_slot(staging_bytes(g));
@@ -713,7 +732,7 @@ int wait_one(b2co_server* s, uint64_t id, b2co_request_info* info)
     }
     if (info) *info = r->info;
     int st = r->info.status;
-    delete r;
+    unref(r);  // the dispatcher may still hold it in its queue
     return st == B2CO_OK ? B2CO_OK : fail(st, "request failed");
 }
 
@@ -882,7 +901,7 @@ int b2co_server_destroy(b2co_server* s)
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();  // drains every submitted request first
     s->free_resources();
-    for (auto& kv : s->all) delete kv.second;
+    for (auto& kv : s->all) unref(kv.second);  // never waited for; the drained queue let go of them
     delete s;
     return B2CO_OK;
 }

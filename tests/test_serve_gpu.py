@@ -236,6 +236,47 @@ def test_scheduled_arrivals_and_small_batches():
             srv2.close()
 
 
+def test_waits_in_any_order_while_requests_stay_queued():
+    """Plain mode admits requests out of queue order, so a finished request can
+    stay in the dispatcher's queue after its caller waited for it.  Here the
+    caller waits newest first and submits more in between (new requests may
+    reuse freed memory); every result stays right in both modes, because a
+    request is freed only when the queue and the caller have both let it go."""
+    import b2co
+    contents = initial_contents()
+    reqs = [r for r in make_requests(contents, count=120, seed=21) if r[1] == b2co.OP_FIND]
+    e_out, _, _ = expected(contents, reqs, b2co.valid_capacity(1_000_000))
+    tables = make_tables(contents)
+    half = len(reqs) // 2
+    for plain in (True, False):
+        srv = b2co.Server(max_inflight=4, hbm_budget_bytes=8 << 30)
+        srv.set_plain(plain)
+        for m in tables:
+            srv.register(m)
+        ins, outs, ids = [], [], []
+        at = b2co.Server.now_ns() + 10_000_000
+
+        def submit(i):
+            t, op, data = reqs[i]
+            inp = b2co.pinned(data.shape, np.int64)
+            inp[...] = data
+            out = b2co.pinned((len(data),), np.int64)
+            ins.append(inp)
+            outs.append(out)
+            ids.append(srv.submit(tables[t], op, inp, out, arrival_ns=at))
+
+        for i in range(half):
+            submit(i)
+        for k in range(half):
+            srv.wait(ids[half - 1 - k])
+            submit(half + k)
+        for rid in ids[half:]:
+            srv.wait(rid)
+        srv.close()
+        for i in range(len(reqs)):
+            assert np.array_equal(outs[i], e_out[i]), (plain, i)
+
+
 def test_budget_admission():
     import b2co
     import torch

@@ -331,8 +331,8 @@ def test_find_host_buffers_match_device_find():
 
 
 def test_window_gather_measurement_aid():
-    """The bare window-read measurement runs over 16-byte-slot tables only,
-    leaves the table unchanged and keeps the batch bound."""
+    """The bare window-read measurement runs over 16- and 8-byte-slot tables,
+    leaves the table unchanged, keeps the batch bound and refuses other slots."""
     import b2co
     import torch
     rng = np.random.default_rng(4)
@@ -345,6 +345,13 @@ def test_window_gather_measurement_aid():
     assert np.array_equal(t.dump_slots(), before)
     with pytest.raises(b2co.LengthError):
         t.window_gather((1 << 31) + 1)
-    s = make_table(8, 0, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, 1 << 12)
+    m = make_table(4, 4, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, 1 << 16)
+    k4 = unique_keys(rng, 20000, 4).astype(np.int32)
+    m.Insert(make_pairs(k4, k4))
+    before = m.dump_slots()
+    m.window_gather(1 << 20, seed=5)
+    torch.cuda.synchronize()
+    assert np.array_equal(m.dump_slots(), before)
+    s = make_table(4, 0, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, 1 << 12)
     with pytest.raises(b2co.InvalidArgument):
         s.window_gather(1024)
