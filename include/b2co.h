@@ -137,7 +137,7 @@ int b2co_oa_data(const b2co_oa_table* table, void** slots);
 int b2co_oa_describe(const b2co_oa_table* table, b2co_oa_desc* desc);
 /* Measurement aid (no reference counterpart): `n` (<= 2^31) reads of whole
  * bucket windows at pseudo-random bucket starts (`seed`) of the table's own
- * slots, four lanes per window, nothing written.  16- or 8-byte slots.  Timing it
+ * slots (16- or 8-byte), four lanes per window, nothing written.  Timing it
  * gives the random-window read rate a lookup's first windows can reach on this
  * GPU, the practical ceiling of Find beside the HBM copy peak. */
 int b2co_oa_window_gather(const b2co_oa_table* table, uint64_t n, uint32_t seed, b2co_stream stream);

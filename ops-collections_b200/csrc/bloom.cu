@@ -255,10 +255,21 @@ __global__ void __launch_bounds__(1024) k_bloom_scan(uint32_t const* totals, uin
     if (t == 1023 && nslices == kMaxSlices) offsets[nslices] = run;
 }
 
-// Shared memory of one route CTA: the tile's records and their destinations,
-// then per slice the tile's count, its offset in the tile, its run's global
-// start, the CTA's running cursor and the slice's end in the workspace.
-constexpr size_t kRouteSmem = size_t(kRouteTile) * (8 + 4) + size_t(kMaxSlices) * 4 * 5 + (kRouteThreads / 32 + 1) * 4;
+// Shared memory of one route CTA: the next tile's keys (8 bytes a key), the
+// tile's records and their destinations, then per slice the tile's count, its
+// offset in the tile, its run's global start, the CTA's running cursor and the
+// slice's end in the workspace.
+__host__ __device__ constexpr uint32_t route_bins(uint32_t nslices) { return (nslices + 31) & ~31u; }
+__host__ __device__ constexpr size_t route_smem(uint32_t nslices)
+{
+    return size_t(kRouteTile) * (8 + 8 + 4) + size_t(route_bins(nslices)) * 4 * 5 + (kRouteThreads / 32 + 1) * 4;
+}
+
+template <int KB>
+__device__ __forceinline__ void cp_async_key(void* dst, void const* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(KB) : "memory");
+}
 
 template <int KB>
 __global__ void __launch_bounds__(kRouteThreads) k_bloom_route(uint32_t nblocks, uint64_t seed, void const* keys,
@@ -266,15 +277,17 @@ __global__ void __launch_bounds__(kRouteThreads) k_bloom_route(uint32_t nblocks,
                                                                uint32_t nctas, uint32_t const* prefix,
                                                                uint32_t const* offsets, unsigned long long* recs)
 {
-    extern __shared__ __align__(16) unsigned char route_smem[];
-    auto* stage = reinterpret_cast<unsigned long long*>(route_smem);
+    extern __shared__ __align__(16) unsigned char route_smem_[];
+    auto* kbuf = reinterpret_cast<unsigned long long*>(route_smem_);  // one 8-byte cell a key
+    auto* stage = kbuf + kRouteTile;
     auto* stage_at = reinterpret_cast<uint32_t*>(stage + kRouteTile);
+    uint32_t const nbins = route_bins(nslices);
     uint32_t* hist = stage_at + kRouteTile;
-    uint32_t* loff = hist + kMaxSlices;
-    uint32_t* gbase = loff + kMaxSlices;
-    uint32_t* gcur = gbase + kMaxSlices;
-    uint32_t* gend = gcur + kMaxSlices;
-    uint32_t* warp_tot = gend + kMaxSlices;  // kRouteThreads / 32 warp sums, then the tile's total
+    uint32_t* loff = hist + nbins;
+    uint32_t* gbase = loff + nbins;
+    uint32_t* gcur = gbase + nbins;
+    uint32_t* gend = gcur + nbins;
+    uint32_t* warp_tot = gend + nbins;  // kRouteThreads / 32 warp sums, then the tile's total
     uint32_t const t = threadIdx.x, lane = t & 31, warp = t >> 5;
     constexpr uint32_t kNone = 0xffffffffu;
     constexpr int kWarps = kRouteThreads / 32;
@@ -285,12 +298,20 @@ __global__ void __launch_bounds__(kRouteThreads) k_bloom_route(uint32_t nblocks,
     }
     uint64_t begin, end;
     route_chunk(n, blockIdx.x, nctas, begin, end);
+    // a thread copies its own keys of the next tile into its own cells while the
+    // CTA works on this tile (cp.async), so key loads never stall a tile
+    auto prefetch = [&](uint64_t b) {
+#pragma unroll
+        for (int j = 0; j < kRouteKeys; ++j) {
+            uint64_t const i = b + uint64_t(j) * kRouteThreads + t;
+            if (i < end) cp_async_key<KB>(kbuf + j * kRouteThreads + t, static_cast<char const*>(keys) + i * KB);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    if (begin < end) prefetch(begin);
     for (uint64_t base = begin; base < end; base += kRouteTile) {
         for (uint32_t i = t; i < nslices; i += kRouteThreads) hist[i] = 0;
-        __syncthreads();
-        // every key of the thread is loaded before any shared-memory atomic, so
-        // the loads are in flight together; a record's rank within its slice
-        // comes from the shared histogram
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
         unsigned long long rec[kRouteKeys];
         uint32_t where[kRouteKeys];  // slice << 16 | rank in the tile, or kNone
         uint64_t key[kRouteKeys];
@@ -299,8 +320,12 @@ __global__ void __launch_bounds__(kRouteThreads) k_bloom_route(uint32_t nblocks,
         for (int j = 0; j < kRouteKeys; ++j) {
             uint64_t const i = base + uint64_t(j) * kRouteThreads + t;
             live[j] = i < end && (!stencil || stencil[i]);
-            key[j] = live[j] ? load_key<KB>(keys, i) : 0;
+            unsigned long long const cell = kbuf[j * kRouteThreads + t];
+            key[j] = live[j] ? (KB == 8 ? cell : uint64_t(uint32_t(cell))) : 0;
         }
+        if (base + kRouteTile < end) prefetch(base + kRouteTile);  // each thread reuses only its own cells
+        __syncthreads();
+        // a record's rank within its slice comes from the shared histogram
 #pragma unroll
         for (int j = 0; j < kRouteKeys; ++j) {
             uint32_t block, lower;
@@ -655,11 +680,12 @@ int launch_add_partitioned(b2co_bloom* f, void const* keys, uint8_t const* stenc
     auto const route = k_bloom_route<KB>;
     auto const count = k_bloom_count<KB>;
     size_t const apply_smem = size_t(kSliceBlocks) * 32;
-    B2CO_CUDA(cudaFuncSetAttribute((void const*)route, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kRouteSmem)));
+    size_t const rsmem = route_smem(nslices);
+    B2CO_CUDA(cudaFuncSetAttribute((void const*)route, cudaFuncAttributeMaxDynamicSharedMemorySize, int(rsmem)));
     B2CO_CUDA(cudaFuncSetAttribute((void const*)k_bloom_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(apply_smem)));
     int per_sm = 0;
-    B2CO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)route, kRouteThreads, kRouteSmem));
+    B2CO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)route, kRouteThreads, rsmem));
     uint32_t const route_cap = uint32_t(per_sm < 1 ? 1 : per_sm) * uint32_t(sm_count());
     // counts[route CTA][slice], then the slice totals and offsets
     size_t const part_words = size_t(route_cap) * kMaxSlices + 2 * size_t(kMaxSlices) + 1;
@@ -682,7 +708,7 @@ int launch_add_partitioned(b2co_bloom* f, void const* keys, uint8_t const* stenc
         count<<<nctas, 1024, 0, s>>>(nblocks, f->seed, k, st, m, nslices, nctas, counts);
         k_bloom_colscan<<<(nslices + 255) / 256, 256, 0, s>>>(counts, nslices, nctas, totals);
         k_bloom_scan<<<1, 1024, 0, s>>>(totals, nslices, offsets);
-        route<<<nctas, kRouteThreads, kRouteSmem, s>>>(nblocks, f->seed, k, st, m, nslices, nctas, counts, offsets,
+        route<<<nctas, kRouteThreads, rsmem, s>>>(nblocks, f->seed, k, st, m, nslices, nctas, counts, offsets,
                                                       f->recs);
         k_bloom_apply<<<nslices, kApplyThreads, apply_smem, s>>>(f->words, nblocks, f->recs, offsets);
     }
@@ -695,6 +721,8 @@ int add_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_s
     if (int st = check(f)) return st;
     if (n == 0) return B2CO_OK;
     if (!keys) return fail(B2CO_EINVAL, "BloomFilter::Add: keys must not be null when keyNum is non-zero");
+    if (reinterpret_cast<uintptr_t>(keys) % f->key_bytes)
+        return fail(B2CO_EINVAL, "BloomFilter::Add: keys must be aligned to the key size");
     if (use_stencil && !stencil)
         return fail(B2CO_EINVAL, "BloomFilter::AddIf: stencil must not be null when keyNum is non-zero");
     if (!f->default_policy())
