@@ -421,8 +421,32 @@ def measure_e2e(t, q, out, stream, world, args):
     floor_ms = pcie_floor_ms(hq, ho, q, out)
     return {"value": round(world * N_QUERIES / (e2e_ms / 1e3) / 1e9, 4), "unit": UNIT,
             "h2d_bytes_per_step": N_QUERIES * 8, "d2h_bytes_per_step": N_QUERIES * 8,
-            "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": (N_QUERIES + (1 << 22) - 1) >> 22,
+            "ms_per_step": round(e2e_ms, 3), "gpu_launches_per_step": host_find_chunks(N_QUERIES),
             "pcie_floor_ms": round(floor_ms, 3), "frac_of_pcie_floor": round(floor_ms / e2e_ms, 4)}
+
+
+def host_find_chunks(n, full=1 << 22):
+    """Chunks (one Find launch each) of the host-buffer Find of n keys: batches
+    of 16 Mi keys or more ramp up with 1 and 2 Mi chunks and down with 2 and 1 Mi."""
+    q, h, off, count = full // 4, full // 2, 0, 0
+    while off < n:
+        left = n - off
+        if n < 4 * full:
+            m = min(left, full)
+        elif off == 0:
+            m = q
+        elif off == q:
+            m = h
+        elif left <= q:
+            m = left
+        elif left <= q + h:
+            m = left - q
+        elif left <= q + h + full:
+            m = left - q - h
+        else:
+            m = full
+        off, count = off + m, count + 1
+    return count
 
 
 def pcie_floor_ms(hq, ho, q, out):

@@ -328,6 +328,14 @@ def test_find_host_buffers_match_device_find():
     out = out_buf(len(q), 8, 8)
     t.Find(dev(q), out)
     assert np.array_equal(pinned_o.numpy(), out.cpu().numpy())
+    # a batch of 16 Mi keys or more ramps its chunk sizes up and down (1, 2, 4, ..., 2, 1 Mi keys)
+    big = q[rng.integers(0, len(q), size=(17 << 20) + 5)]
+    pinned_q = torch.from_numpy(big).pin_memory()
+    pinned_o = torch.empty(len(big), dtype=torch.int64).pin_memory()
+    t.FindHost(pinned_q.numpy(), pinned_o.numpy())
+    out = out_buf(len(big), 8, 8)
+    t.Find(dev(big), out)
+    assert np.array_equal(pinned_o.numpy(), out.cpu().numpy())
 
 
 def test_window_gather_measurement_aid():
