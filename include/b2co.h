@@ -168,7 +168,9 @@ int b2co_oa_insert_or_assign_async(b2co_oa_table* table, const void* pairs, uint
 int b2co_oa_assign_if_async(b2co_oa_table* table, const void* pairs, const uint8_t* stencil, uint64_t n,
                             b2co_stream stream);
 /* InsertAndFind: per input the found payload (T[n]; the key for sets) and a
- * 1-byte inserted flag.
+ * 1-byte inserted flag.  First-wins batches use scratch owned by the table;
+ * asynchronous first-wins calls on different streams run on the GPU one after
+ * the other, in call order (not while a stream is being captured).
  * reference: static_map.h:256 InsertAndFind, :273 InsertAndFindAsync, open_addressing_impl.h:220-234, kernels.h:212-245. */
 int b2co_oa_insert_and_find(b2co_oa_table* table, const void* pairs, void* out_found, uint8_t* out_inserted,
                             uint64_t n, int mode, b2co_stream stream);
@@ -569,6 +571,9 @@ typedef enum {
     B2CO_BLOOM_ADD_AUTO = 3
 } b2co_bloom_add_mode;
 int b2co_bloom_set_add_mode(b2co_bloom* filter, int mode);
+/* Asynchronous partitioned Adds on different streams share the filter's
+ * workspace and run on the GPU one after the other, in call order (not while
+ * a stream is being captured); the other Add modes need no ordering. */
 int b2co_bloom_add_async(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream stream);
 int b2co_bloom_add_if(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint64_t n, b2co_stream stream);
 int b2co_bloom_add_if_async(b2co_bloom* filter, const void* keys, const uint8_t* stencil, uint64_t n,

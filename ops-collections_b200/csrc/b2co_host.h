@@ -30,6 +30,19 @@ int sm_count();
 // items per block, capped at the blocks that can be resident at once.
 uint32_t grid_for(void const* kernel, uint32_t block, uint64_t work, uint64_t per_block);
 
+// Orders the uses of one piece of library-owned scratch (first-wins
+// InsertAndFind's, the routed Bloom Add's workspace) across the callers'
+// streams: a use waits on the GPU for the previous use to end, so async calls
+// on different streams cannot interleave on it.  While a stream is being
+// captured into a graph nothing is added (the graph's own order holds).
+struct ScratchOrder {
+    cudaEvent_t done = nullptr;
+    bool used = false;
+    int begin(cudaStream_t s);  // before the first launch that touches the scratch
+    int end(cudaStream_t s);    // after the last one
+    void release();
+};
+
 // Largest batch a single launch accepts: 32-bit indices plus one grid stride
 // must not overflow (the reference's CheckedBatchSize,
 // detail/open_addressing/open_addressing_impl.h:534-545).

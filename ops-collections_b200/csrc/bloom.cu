@@ -590,6 +590,7 @@ struct b2co_bloom {
     uint64_t recs_cap = 0;
     uint32_t* part = nullptr;  // partitioned Add: per-CTA slice counts, slice totals and offsets
     size_t part_words = 0;
+    ScratchOrder part_order;  // the workspace serves one partitioned Add at a time
     uint64_t num_blocks = 0;
     uint32_t key_bytes = 0;
     uint64_t seed = 0;
@@ -699,6 +700,7 @@ int launch_add_partitioned(b2co_bloom* f, void const* keys, uint8_t const* stenc
     uint32_t* counts = f->part;
     uint32_t* totals = counts + size_t(route_cap) * kMaxSlices;
     uint32_t* offsets = totals + kMaxSlices;
+    if (int st = f->part_order.begin(s)) return st;
     for (uint64_t at = 0; at < n; at += kPartitionRound) {
         uint64_t const m = n - at < kPartitionRound ? n - at : kPartitionRound;
         void const* k = static_cast<char const*>(keys) + at * KB;
@@ -713,7 +715,7 @@ int launch_add_partitioned(b2co_bloom* f, void const* keys, uint8_t const* stenc
         k_bloom_apply<<<nslices, kApplyThreads, apply_smem, s>>>(f->words, nblocks, f->recs, offsets);
     }
     B2CO_CUDA(cudaGetLastError());
-    return B2CO_OK;
+    return f->part_order.end(s);
 }
 
 int add_impl(b2co_bloom* f, void const* keys, uint8_t const* stencil, bool use_stencil, uint64_t n, cudaStream_t s)
@@ -839,6 +841,7 @@ int b2co_bloom_destroy(b2co_bloom* f)
     if (f->words) cudaFree(f->words);
     if (f->recs) cudaFree(f->recs);
     if (f->part) cudaFree(f->part);
+    f->part_order.release();
     delete f;
     return B2CO_OK;
 }

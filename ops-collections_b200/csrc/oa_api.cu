@@ -62,6 +62,7 @@ struct b2co_oa_table {
     // first-wins InsertAndFind scratch, grown on demand
     uint32_t* d_pos = nullptr;
     uint64_t pos_cap = 0;
+    ScratchOrder first_wins_order;  // pos, the two bitmaps and owner[] serve one batch at a time
     uint32_t* d_newbits = nullptr;
     uint32_t* d_owner = nullptr;
     // host-buffer Find pipeline
@@ -372,6 +373,7 @@ int b2co_oa_destroy(b2co_oa_table* t)
     if (t->d_pos) cudaFree(t->d_pos);
     if (t->d_newbits) cudaFree(t->d_newbits);
     if (t->d_owner) cudaFree(t->d_owner);
+    t->first_wins_order.release();
     if (t->stage) cudaFree(t->stage);
     for (auto& s : t->pipe)
         if (s) cudaStreamDestroy(s);
@@ -509,9 +511,12 @@ int b2co_oa_insert_and_find_async(b2co_oa_table* t, void const* pairs, void* out
         return t->ops->iaf_race(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), cs(s));
     if (mode != B2CO_IAF_FIRST_WINS) return fail(B2CO_EINVAL, "unknown InsertAndFind mode");
     if (int st = ensure_first_wins_scratch(t, n)) return st;
+    if (int st = t->first_wins_order.begin(cs(s))) return st;
     B2CO_CUDA(cudaMemsetAsync(t->d_newbits, 0, ((t->capacity + 31) / 32) * 8, cs(s)));
-    return t->ops->iaf_first(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n), t->d_pos,
-                             t->d_newbits, t->d_owner, cs(s));
+    if (int st = t->ops->iaf_first(t->args, t->desc.bucket_size, pairs, out_found, out_inserted, uint32_t(n),
+                                   t->d_pos, t->d_newbits, t->d_owner, cs(s)))
+        return st;
+    return t->first_wins_order.end(cs(s));
 }
 
 int b2co_oa_reserve_insert_and_find(b2co_oa_table* t, uint64_t n)

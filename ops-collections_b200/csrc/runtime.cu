@@ -25,6 +25,41 @@ int cuda_fail(cudaError_t e, char const* what)
                 std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
 }
 
+namespace {
+bool capturing(cudaStream_t s)
+{
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return st != cudaStreamCaptureStatusNone;
+}
+}  // namespace
+
+int ScratchOrder::begin(cudaStream_t s)
+{
+    if (capturing(s)) return B2CO_OK;
+    if (!done) B2CO_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    if (used) B2CO_CUDA(cudaStreamWaitEvent(s, done, 0));
+    return B2CO_OK;
+}
+
+int ScratchOrder::end(cudaStream_t s)
+{
+    if (capturing(s) || !done) return B2CO_OK;
+    B2CO_CUDA(cudaEventRecord(done, s));
+    used = true;
+    return B2CO_OK;
+}
+
+void ScratchOrder::release()
+{
+    if (done) cudaEventDestroy(done);
+    done = nullptr;
+    used = false;
+}
+
 int sm_count()
 {
     static int cached[64] = {0};

@@ -50,6 +50,29 @@ def test_bloom_add_contains_bit_exact(kdt, num_blocks, mode):
     assert np.array_equal(out.cpu().numpy(), oracle.bloom_contains(words, num_blocks, q) & st)
 
 
+def test_partitioned_adds_on_two_streams_share_the_workspace_in_order():
+    """Two asynchronous routed Adds on different streams use the filter's one
+    workspace one after the other; the bits are the oracle's for both batches."""
+    import b2co
+    import torch
+    rng = np.random.default_rng(31)
+    nb = 5000
+    ka = rng.integers(0, 2**63, size=400000, dtype=np.uint64)
+    kb = rng.integers(0, 2**63, size=300000, dtype=np.uint64)
+    f = b2co.BloomFilter(nb, key_dtype=torch.int64)
+    f.set_add_mode(b2co.BLOOM_ADD_PARTITIONED)
+    da, db = dev(ka.view(np.int64)), dev(kb.view(np.int64))
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()
+    f.AddAsync(da, stream=s1)
+    f.AddAsync(db, stream=s2)
+    torch.cuda.synchronize()
+    words = np.zeros(nb * 8, dtype=np.uint32)
+    oracle.bloom_add(words, nb, ka)
+    oracle.bloom_add(words, nb, kb)
+    assert np.array_equal(f.words(), words)
+
+
 def test_bloom_add_if_merge_intersect_and_errors():
     import b2co
     import torch

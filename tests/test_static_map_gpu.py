@@ -132,6 +132,37 @@ def test_insert_and_find_first_wins_matches_sequential(layout, scheme):
     assert np.array_equal(got, o.pairs())
 
 
+def test_first_wins_batches_on_two_streams_apply_in_call_order():
+    """Two asynchronous first-wins batches on different streams share the
+    table's scratch: the second waits on the GPU for the first, so the result
+    is the two batches applied in call order."""
+    import b2co
+    import torch
+    rng = np.random.default_rng(77)
+    keys = unique_keys(rng, 300000, 8)
+    a_keys = np.concatenate([keys[:200000], keys[:20000]])
+    b_keys = np.concatenate([keys[100000:], keys[150000:170000]])
+    rng.shuffle(a_keys)
+    rng.shuffle(b_keys)
+    a_vals, b_vals = values_for(rng, a_keys, 8), values_for(rng, b_keys, 8)
+    t = make_table(8, 8, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32, 600000)
+    o = oracle_table(t, 8, 8, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32)
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    fa, ia = out_buf(len(a_keys), 8, 8), torch.empty(len(a_keys), dtype=torch.uint8, device="cuda")
+    fb, ib = out_buf(len(b_keys), 8, 8), torch.empty(len(b_keys), dtype=torch.uint8, device="cuda")
+    pa, pb = make_pairs(a_keys, a_vals), make_pairs(b_keys, b_vals)
+    torch.cuda.synchronize()
+    t.InsertAndFindAsync(pa, fa, ia, stream=s1, mode=b2co.IAF_FIRST_WINS)
+    t.InsertAndFindAsync(pb, fb, ib, stream=s2, mode=b2co.IAF_FIRST_WINS)
+    torch.cuda.synchronize()
+    ef, ei = o.insert_and_find(a_keys, a_vals)
+    assert np.array_equal(ia.cpu().numpy(), ei) and np.array_equal(fa.cpu().numpy(), ef)
+    ef, ei = o.insert_and_find(b_keys, b_vals)
+    assert np.array_equal(ib.cpu().numpy(), ei) and np.array_equal(fb.cpu().numpy(), ef)
+    got, _ = stored_pairs(t, 8, 8, 5, oracle.PROBE_DOUBLE, oracle.HASH_XXH32)
+    assert np.array_equal(got, o.pairs())
+
+
 @pytest.mark.parametrize("layout", LAYOUTS, ids=lambda l: f"k{l[0]}v{l[1]}")
 def test_insert_and_find_race_invariants(layout):
     """insert_and_find_test.cpp:106-147: one winner per key and every
