@@ -77,11 +77,7 @@ __device__ __forceinline__ void hll_locate_p(uint64_t key, uint32_t& index, uint
 {
     uint64_t const h = xxh64<KB>(key, 0);
     index = uint32_t(h >> (64 - P));
-    // the rank's leading zeros almost always end within the high word (the
-    // whole 64-bit count only when its 32 - P bits after the index are zero)
-    uint32_t const top = uint32_t(h >> 32) << P;
-    if (__builtin_expect(top != 0, 1)) rank = uint32_t(__clz(int(top))) + 1u;
-    else rank = uint32_t(__clzll((long long)((h << P) | (1ull << (P - 1))))) + 1u;
+    rank = uint32_t(__clzll((long long)((h << P) | (1ull << (P - 1))))) + 1u;
 }
 
 constexpr int kHllBlock = 1024;
