@@ -629,7 +629,8 @@ int b2co_hll_bias_data(uint32_t precision, const double** raw_estimates, const d
 
 typedef struct b2co_dmap b2co_dmap;
 
-/* reference: include/dynamic_map.h:94-133 (emptyKey == erasedKey -> EINVAL). */
+/* reference: include/dynamic_map.h:94-133 (emptyKey == erasedKey -> EINVAL).
+ * Key types and slot layouts as for StaticMap (the submaps check them). */
 int b2co_dmap_create(const b2co_oa_desc* desc, uint64_t initial_capacity, b2co_stream stream, b2co_dmap** out);
 int b2co_dmap_destroy(b2co_dmap* map);
 /* reference: dynamic_map.h:137-139 Size / Capacity / NumSubmaps. */

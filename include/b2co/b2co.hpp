@@ -379,9 +379,9 @@ class StaticSet : public detail::OpenAddressing<Key, Key, ExtentT, KeyEqual, Pro
 template <class Key, class T, class ExtentT = Extent<std::size_t>, class KeyEqual = EqualTo<Key>,
           class ProbingScheme = LinearProbing<murmurhash3_32<Key>>, class StorageT = Storage<5>>
 class DynamicMap {
-    static_assert(!detail::is_float_key<Key> && (sizeof(Key) == 4 || sizeof(Key) == 8) &&
-                      (sizeof(T) == 4 || sizeof(T) == 8),
-                  "DynamicMap takes 4- or 8-byte integer keys and 4- or 8-byte payloads");
+    static_assert(sizeof(Key) == 2 || sizeof(Key) == 4 || sizeof(Key) == 8, "keys are 2, 4 or 8 bytes");
+    static_assert(sizeof(Key) == 2 ? sizeof(T) == 2 : (sizeof(T) == 4 || sizeof(T) == 8),
+                  "2-byte keys take 2-byte payloads; wider keys take 4- or 8-byte payloads");
 
    public:
     using SizeType = typename ExtentT::ValueType;
@@ -398,6 +398,7 @@ class DynamicMap {
         d.bucket_size = StorageT::bucketSize;
         d.probing = ProbingScheme::probing;
         d.hash = ProbingScheme::hash;
+        d.key_kind = detail::is_float_key<Key> ? B2CO_KEY_FLOAT : B2CO_KEY_INTEGER;
         d.empty_key_bits = detail::bits_of(emptyKey);
         d.empty_value_bits = detail::bits_of(emptyValue);
         d.erased_key_bits = detail::bits_of(erasedKey);

@@ -637,8 +637,9 @@ class DynamicMap:
         value_dtype = value_dtype or torch.int32
         kb, vb = _dtype_bytes(key_dtype), _dtype_bytes(value_dtype)
         self.key_bytes, self.value_bytes = kb, vb
-        d = OaDesc(kb, vb, bucket_size, probing, hash_kind, 0, _bits(empty_key, kb), _bits(empty_value, vb),
-                   _bits(erased_key, kb))
+        fk, fv = _is_float(key_dtype), _is_float(value_dtype)
+        d = OaDesc(kb, vb, bucket_size, probing, hash_kind, KEY_FLOAT if fk else KEY_INTEGER, _bits(empty_key, kb, fk),
+                   _bits(empty_value, vb, fv), _bits(erased_key, kb, fk))
         h = C.c_void_p()
         _call("b2co_dmap_create", C.byref(d), C.c_uint64(initial_capacity), _stream(stream), C.byref(h))
         self._h = h

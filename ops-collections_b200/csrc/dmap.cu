@@ -110,7 +110,11 @@ struct b2co_dmap {
         if (prep) cudaStreamDestroy(prep);
     }
 
-    uint32_t pair_bytes() const { return desc.value_bytes == 0 ? desc.key_bytes : (desc.key_bytes + desc.value_bytes == 8 ? 8 : 16); }
+    uint32_t pair_bytes() const
+    {
+        uint32_t const raw = desc.key_bytes + desc.value_bytes;
+        return raw <= 4 ? 4 : (raw <= 8 ? 8 : 16);
+    }
     uint64_t capacity_of(size_t i) const
     {
         uint64_t c = 0;
@@ -260,8 +264,9 @@ struct b2co_dmap {
 
     int extract_keys(void const* pairs, uint32_t n, cudaStream_t s)
     {
-        uint32_t kb = desc.key_bytes, vb = desc.value_bytes;
-        if (kb == 4 && vb == 4) launch_extract<SlotT<4, 4>>(d_keys(), pairs, n, s);
+        uint32_t kb = desc.key_bytes, vb = desc.value_bytes;  // the key's bits, whatever its kind
+        if (kb == 2) launch_extract<SlotT<2, 2>>(d_keys(), pairs, n, s);
+        else if (kb == 4 && vb == 4) launch_extract<SlotT<4, 4>>(d_keys(), pairs, n, s);
         else if (kb == 4 && vb == 8) launch_extract<SlotT<4, 8>>(d_keys(), pairs, n, s);
         else if (kb == 8 && vb == 4) launch_extract<SlotT<8, 4>>(d_keys(), pairs, n, s);
         else launch_extract<SlotT<8, 8>>(d_keys(), pairs, n, s);
@@ -369,8 +374,8 @@ int b2co_dmap_create(b2co_oa_desc const* d, uint64_t initial_capacity, b2co_stre
     if (!d || !out) return fail(B2CO_EINVAL, "null descriptor or output");
     *out = nullptr;
     if (d->value_bytes == 0) return fail(B2CO_EINVAL, "DynamicMap needs a payload (value_bytes > 0)");
-    if (d->key_kind != B2CO_KEY_INTEGER || d->key_bytes < 4 || d->value_bytes < 4)
-        return fail(B2CO_EINVAL, "DynamicMap takes 4- or 8-byte integer keys and payloads");
+    // the submaps check the layout and the key kind (2-byte keys with 2-byte
+    // payloads; 4- and 8-byte keys with 4- or 8-byte payloads; integer or float)
     uint64_t kmask = d->key_bytes >= 8 ? ~0ull : ((1ull << (8 * d->key_bytes)) - 1);
     if ((d->empty_key_bits & kmask) == (d->erased_key_bits & kmask))
         return fail(B2CO_EINVAL, "DynamicMap: emptyKey and erasedKey must differ");
@@ -545,8 +550,9 @@ int b2co_dmap_find(b2co_dmap* m, void const* keys, void* out, uint64_t n, b2co_s
         for (size_t i = base + 1; i < m->submaps.size(); ++i) {
             if (!m->sizes[i]) continue;
             if (int st = b2co_oa_find_async(m->submaps[i].get(), keys, m->scratch, n, stream)) return st;
-            int st = vb == 8 ? merge_find<unsigned long long>(out, m->scratch, m->desc.empty_value_bits, n, s)
-                             : merge_find<uint32_t>(out, m->scratch, m->desc.empty_value_bits, n, s);
+            int st = vb == 8   ? merge_find<unsigned long long>(out, m->scratch, m->desc.empty_value_bits, n, s)
+                     : vb == 4 ? merge_find<uint32_t>(out, m->scratch, m->desc.empty_value_bits, n, s)
+                               : merge_find<unsigned short>(out, m->scratch, m->desc.empty_value_bits, n, s);
             if (st) return st;
         }
     }

@@ -91,3 +91,67 @@ def test_dynamic_map_reserve_and_append_unique():
     m.Find(dev(keys), out)
     assert np.array_equal(out.cpu().numpy(), vals)
     assert m.Capacity() >= 200000
+
+
+@pytest.mark.parametrize("kdt,vdt", [(np.int16, np.int16), (np.uint16, np.uint16), (np.float16, np.float16),
+                                     (np.float32, np.float32), (np.float64, np.float64), (np.float32, np.int64)],
+                         ids=lambda d: np.dtype(d).name)
+def test_dynamic_map_two_byte_and_float_keys(kdt, vdt):
+    """The reference's DynamicMap tests instantiate (uint16, uint16) and
+    (float, float) maps (tests/dynamic_map/*_test.cpp).  Growth over several
+    submaps, exact dedup and fan-out Find, checked against a dict; sentinels
+    compare by their bits.  (Signed zeros and NaNs follow the probe: their
+    cases are checked against the oracle in test_key_kinds_gpu.py.)"""
+    import b2co
+    import torch
+    rng = np.random.default_rng(np.dtype(kdt).itemsize * 7 + np.dtype(vdt).itemsize)
+    if np.dtype(kdt).kind == "f":
+        pool = rng.uniform(-1000.0, 1000.0, size=60000).astype(kdt)
+        pool = np.unique(pool[np.isfinite(pool)])
+        pool = pool[(pool != -1.0) & (pool != -2.0) & (pool != 0.0)]
+        keys = np.concatenate([np.array([0.0], dtype=kdt), rng.permutation(pool)[:20000]])
+    else:
+        lo = -30000 if np.dtype(kdt).kind == "i" else 0
+        pool = np.arange(lo, lo + 60000, dtype=np.int64)
+        pool = pool[(pool != -1) & (pool != -2) & (pool != np.iinfo(kdt).max) & (pool != np.iinfo(kdt).max - 1)]
+        keys = rng.permutation(pool)[:20000].astype(kdt)
+    if np.dtype(vdt).kind == "f":
+        vals = rng.uniform(0.0, 100.0, size=len(keys)).astype(vdt)
+    else:
+        vals = rng.integers(1, 20000, size=len(keys)).astype(vdt)
+    to_t = {np.dtype(np.int16): torch.int16, np.dtype(np.uint16): torch.int16, np.dtype(np.float16): torch.float16,
+            np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64,
+            np.dtype(np.int64): torch.int64}
+    ek = -1 if np.dtype(kdt).kind != "u" else np.iinfo(kdt).max
+    xk = -2 if np.dtype(kdt).kind != "u" else np.iinfo(kdt).max - 1
+    m = b2co.DynamicMap(4000, kdt(ek), vdt(-1 if np.dtype(vdt).kind != "u" else 0), kdt(xk),
+                        key_dtype=to_t[np.dtype(kdt)], value_dtype=to_t[np.dtype(vdt)])
+    empty_v = np.array([-1 if np.dtype(vdt).kind != "u" else 0], dtype=vdt)[0]
+    gold = {}
+    off = 0
+    for size in (3000, 5000, 6000, 6001):
+        k, v = keys[off:off + size], vals[off:off + size]
+        if off:  # old keys again (dedup keeps the first payload)
+            k = np.concatenate([k, keys[:500]])
+            v = np.concatenate([v, vals[:500]])
+        got = m.Insert(b2co.pack_pairs(dev(k), dev(v)))
+        new = 0
+        for x, y in zip(k.tolist(), v.tolist()):
+            if x not in gold:
+                gold[x] = y
+                new += 1
+        assert got == new
+        off += size
+    assert m.Size() == len(gold)
+    assert m.NumSubmaps() > 1
+    misses = np.array([x for x in (pool[-3000:] if np.dtype(kdt).kind == "f" else pool[-3000:].astype(kdt))
+                       if x not in gold][:1000], dtype=kdt)
+    q = np.concatenate([keys, misses])
+    out = torch.empty(len(q), dtype=to_t[np.dtype(vdt)], device="cuda")
+    m.Find(dev(q), out)
+    exp = np.array([gold.get(x, empty_v) for x in q.tolist()], dtype=vdt)
+    assert np.array_equal(out.cpu().numpy().view(np.uint8), exp.view(np.uint8))
+    c = torch.empty(len(q), dtype=torch.uint8, device="cuda")
+    m.Contains(dev(q), c)
+    assert np.array_equal(c.cpu().numpy(), np.array([x in gold for x in q.tolist()], dtype=np.uint8))
+
