@@ -811,7 +811,8 @@ def small_map_measurements(stream, reps=200):
     q = np.concatenate([keys[rng.integers(0, n, size=n // 2)], miss])
     rng.shuffle(q)
     exp = np.where(np.isin(q, keys), (2 * q.astype(np.int64) + 1).astype(np.int32), np.int32(-1))
-    t = b2co.StaticMap(2_097_152, -1, -1, key_dtype=torch.int32, value_dtype=torch.int32)
+    t = b2co.StaticMap(2_097_152, -1, -1, key_dtype=torch.int32, value_dtype=torch.int32, bucket_size=5,
+                       probing=b2co.PROBE_DOUBLE, hash_kind=b2co.HASH_XXH32)
     dk, dv, dq = (torch.from_numpy(a).cuda() for a in (keys, vals, q))
     pairs = b2co.pack_pairs(dk, dv)
     out = torch.empty(len(q), dtype=torch.int32, device="cuda")
