@@ -95,19 +95,27 @@ cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Default lookup shape per layout; b2co_oa_set_find_shape overrides it per table.
 // Tables at most this large keep their windows in the 126 MB L2 next to the
-// query stream.
+// query stream (the lookup shapes' crossover was measured at 21 and 42 MB
+// against 4.3 GB).
 constexpr uint64_t kL2ResidentTableBytes = uint64_t(64) << 20;
+// One lane per key also wins for writes to tables up to about twice the L2
+// (1.7x at 70 and 130 MB, 1.45x at 260 MB) and loses from 520 MB on.
+constexpr uint64_t kPerKeyWriteTableBytes = uint64_t(256) << 20;
 
-bool l2_resident(b2co_oa_table const* t)
+uint64_t table_bytes(b2co_oa_table const* t)
 {
-    return uint64_t(t->capacity) * slot_bytes(t->desc.key_bytes, t->desc.value_bytes) <= kL2ResidentTableBytes;
+    return uint64_t(t->capacity) * slot_bytes(t->desc.key_bytes, t->desc.value_bytes);
 }
+bool l2_resident(b2co_oa_table const* t) { return table_bytes(t) <= kL2ResidentTableBytes; }
 
-// Writes to a table that fits in L2 run one lane per key (the reference's scan
-// as written): with windows served from L2, more keys in flight beat
-// cooperative windows (25.5 vs 15.7 Gpairs/s inserting 10^6 pairs into the
+// Writes to tables of up to kPerKeyWriteTableBytes run one lane per key (the
+// reference's scan as written): with most windows served from L2, more keys in
+// flight beat cooperative windows (27.1 vs 15.9 Gpairs/s inserting into the
 // 21 MB int32 table).  Larger tables take the cooperative default.
-void default_write_shape(b2co_oa_table* t) { t->args.write_shape = l2_resident(t) ? (1u << 8) | 1u : 0u; }
+void default_write_shape(b2co_oa_table* t)
+{
+    t->args.write_shape = table_bytes(t) <= kPerKeyWriteTableBytes ? (1u << 8) | 1u : 0u;
+}
 
 void default_shape(b2co_oa_table* t)
 {
