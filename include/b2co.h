@@ -232,8 +232,8 @@ int b2co_oa_find_host(b2co_oa_table* table, const void* host_keys, void* host_ou
  * B2CO_FIND_SEGMENTED (scan each first bucket window by 64-byte segments and
  * read the second segment only when the first does not end the scan) and the
  * flags below; 0, 0 = library default (4 lanes, 2 windows, B2CO_FIND_DEFERRED;
- * 2 lanes, 1 window for 4-byte slots and for tables of at most 64 MiB, which
- * stay in L2).  No reference counterpart (the reference
+ * 2 lanes, 1 window for 4-byte slots and for tables of at most 320 MiB, which
+ * are served mostly from L2).  No reference counterpart (the reference
  * launches one thread per key). */
 #define B2CO_FIND_SEGMENTED 0x100u
 /* OR-ed into keys_per_lane: fetch every first bucket window with one bulk (TMA)
@@ -251,7 +251,7 @@ int b2co_oa_set_find_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_
  * as written); 2, 4 or 8 lanes share each bucket window with keys_per_tile
  * (1, 2 or 4) keys in flight per lane group.  (0, 0) restores the default:
  * 4 lanes, 1 key (one lane per key for bucket size 1 and for tables of at
- * most 256 MiB, whose windows mostly come from L2).  Layouts with 2-byte
+ * most 320 MiB, whose windows mostly come from L2).  Layouts with 2-byte
  * or floating-point keys run the default window shape for any request other
  * than one lane per key. */
 int b2co_oa_set_write_shape(b2co_oa_table* table, uint32_t lanes_per_key, uint32_t keys_per_tile);

@@ -94,28 +94,22 @@ int check_batch(uint64_t n)
 cudaStream_t cs(b2co_stream s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Default lookup shape per layout; b2co_oa_set_find_shape overrides it per table.
-// Tables at most this large keep their windows in the 126 MB L2 next to the
-// query stream (the lookup shapes' crossover was measured at 21 and 42 MB
-// against 4.3 GB).
-constexpr uint64_t kL2ResidentTableBytes = uint64_t(64) << 20;
-// One lane per key also wins for writes to tables up to about twice the L2
-// (1.7x at 70 and 130 MB, 1.45x at 260 MB) and loses from 520 MB on.
-constexpr uint64_t kPerKeyWriteTableBytes = uint64_t(256) << 20;
+// Tables at most this large (about 2.5 times the 126 MB L2) are served mostly
+// from L2, and the keys in flight per warp set their rate: measured on int64
+// tables, two-lane lookups beat four-lane ones by 1.39x at 70 MB, 1.17x at 130 MB
+// and 1.21x at 260 MB and lose by 8% at 520 MB; one-lane-per-key writes win by
+// 1.7x at 70 and 130 MB and 1.45x at 260 MB and lose by 11% at 520 MB.
+constexpr uint64_t kSmallTableBytes = uint64_t(320) << 20;
 
 uint64_t table_bytes(b2co_oa_table const* t)
 {
     return uint64_t(t->capacity) * slot_bytes(t->desc.key_bytes, t->desc.value_bytes);
 }
-bool l2_resident(b2co_oa_table const* t) { return table_bytes(t) <= kL2ResidentTableBytes; }
+bool small_table(b2co_oa_table const* t) { return table_bytes(t) <= kSmallTableBytes; }
 
-// Writes to tables of up to kPerKeyWriteTableBytes run one lane per key (the
-// reference's scan as written): with most windows served from L2, more keys in
-// flight beat cooperative windows (27.1 vs 15.9 Gpairs/s inserting into the
-// 21 MB int32 table).  Larger tables take the cooperative default.
-void default_write_shape(b2co_oa_table* t)
-{
-    t->args.write_shape = table_bytes(t) <= kPerKeyWriteTableBytes ? (1u << 8) | 1u : 0u;
-}
+// Writes to small tables run one lane per key (the reference's scan as
+// written); larger tables take the cooperative default.
+void default_write_shape(b2co_oa_table* t) { t->args.write_shape = small_table(t) ? (1u << 8) | 1u : 0u; }
 
 void default_shape(b2co_oa_table* t)
 {
@@ -126,12 +120,10 @@ void default_shape(b2co_oa_table* t)
         // keys staged per warp, keys that probe on past their first window
         // queued and followed a pass at a time; four lanes per window (a 64-byte
         // row of 16-byte slots per load) with two windows in flight, or two
-        // lanes and one window for 4-byte slots and for tables that fit in L2
-        // (measured best per layout and size: windows served from L2 come back
-        // fast enough that keys in flight per warp, not requests per window,
-        // set the rate -- 1.6x on 21 and 42 MB tables, and slower on HBM tables)
+        // lanes and one window for 4-byte slots and for small tables (measured
+        // best per layout and size, see kSmallTableBytes)
         uint32_t const sb = slot_bytes(t->desc.key_bytes, t->desc.value_bytes);
-        bool const narrow = sb <= 4 || l2_resident(t);
+        bool const narrow = sb <= 4 || small_table(t);
         t->find_lanes = narrow ? 2 : 4;
         t->find_items = (narrow ? 1 : 2) | kShapeDeferred;
     }
