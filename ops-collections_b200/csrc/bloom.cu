@@ -464,24 +464,38 @@ __global__ void __launch_bounds__(256) k_bloom_contains(uint32_t const* words, u
                                                         void const* keys, uint8_t const* stencil, uint8_t* out,
                                                         uint64_t n)
 {
-    uint64_t const stride = uint64_t(gridDim.x) * blockDim.x;
-    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
-        uint8_t r = 0;
-        if (!stencil || stencil[i]) {
-            uint32_t block, lower;
-            locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower);
-            uint4 const* p = reinterpret_cast<uint4 const*>(words + uint64_t(block) * 8);
-            uint4 a = __ldg(p), b = __ldg(p + 1);
-            uint32_t const w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-            bool all = true;
+    // kKeys keys per thread and pass, each pass's block loads issued before any
+    // is tested, so a thread keeps that many random sector reads in flight
+    constexpr int kKeys = 4;
+    uint64_t const tile = uint64_t(blockDim.x) * kKeys;
+    for (uint64_t base = uint64_t(blockIdx.x) * tile; base < n; base += uint64_t(gridDim.x) * tile) {
+        uint32_t lower[kKeys];
+        bool live[kKeys];
+        uint4 lo[kKeys], hi[kKeys];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                uint32_t bit = word_bit(j, lower);
-                all &= (w[j] & bit) == bit;
-            }
-            r = all;
+        for (int j = 0; j < kKeys; ++j) {
+            uint64_t const i = base + uint64_t(j) * blockDim.x + threadIdx.x;
+            live[j] = i < n && (!stencil || stencil[i]);
+            uint32_t block = 0;
+            lower[j] = 0;
+            if (live[j]) locate<KB>(load_key<KB>(keys, i), seed, nblocks, block, lower[j]);
+            uint4 const* p = reinterpret_cast<uint4 const*>(words + uint64_t(block) * 8);
+            lo[j] = live[j] ? __ldg(p) : make_uint4(0u, 0u, 0u, 0u);
+            hi[j] = live[j] ? __ldg(p + 1) : make_uint4(0u, 0u, 0u, 0u);
         }
-        out[i] = r;
+#pragma unroll
+        for (int j = 0; j < kKeys; ++j) {
+            uint64_t const i = base + uint64_t(j) * blockDim.x + threadIdx.x;
+            if (i >= n) continue;
+            uint32_t const w[8] = {lo[j].x, lo[j].y, lo[j].z, lo[j].w, hi[j].x, hi[j].y, hi[j].z, hi[j].w};
+            bool all = live[j];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                uint32_t const bit = word_bit(k, lower[j]);
+                all &= (w[k] & bit) == bit;
+            }
+            out[i] = all;
+        }
     }
 }
 
