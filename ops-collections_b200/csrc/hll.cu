@@ -299,18 +299,22 @@ int add_launch(b2co_hll* h, void const* keys, uint64_t n, cudaStream_t s)
              k_hll_add_vec<4, 17>},
             {k_hll_add_vec<8, 13>, k_hll_add_vec<8, 14>, k_hll_add_vec<8, 15>, k_hll_add_vec<8, 16>,
              k_hll_add_vec<8, 17>}};
-        static int per_sm_cache[2][5] = {};
-        int const ki = h->key_bytes == 8, pi = int(p) - 13;
+        // the shared-memory opt-in is a per-device function attribute: set it on
+        // every launch (it costs about a microsecond), cache only the occupancy
+        constexpr int kDevices = 64;
+        static int per_sm_cache[kDevices][2][5] = {};
+        int const ki = h->key_bytes == 8, pi = int(p) - 13, dev = h->device;
         AddFn const k = fns[ki][pi];
         size_t const smem = size_t(1) << p;
-        if (!per_sm_cache[ki][pi]) {
-            B2CO_CUDA(cudaFuncSetAttribute((void const*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-            int per_sm = 0;
+        B2CO_CUDA(cudaFuncSetAttribute((void const*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int per_sm = dev >= 0 && dev < kDevices ? per_sm_cache[dev][ki][pi] : 0;
+        if (!per_sm) {
             B2CO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)k, kHllBlock, smem));
-            per_sm_cache[ki][pi] = per_sm < 1 ? 1 : per_sm;
+            if (per_sm < 1) per_sm = 1;
+            if (dev >= 0 && dev < kDevices) per_sm_cache[dev][ki][pi] = per_sm;
         }
         uint64_t const want = (n + uint64_t(kHllBlock) * 16 - 1) / (uint64_t(kHllBlock) * 16);  // >= ~16 keys a thread
-        uint64_t const cap = uint64_t(per_sm_cache[ki][pi]) * sm_count();
+        uint64_t const cap = uint64_t(per_sm) * sm_count();
         uint32_t const grid = uint32_t(want < 1 ? 1 : (want < cap ? want : cap));
         // keys up to the first 16-byte boundary go one per thread
         uintptr_t const addr = reinterpret_cast<uintptr_t>(keys);

@@ -215,12 +215,10 @@ struct OaImpl {
         if constexpr (S::bytes == 16) {
             auto k = k_find_bulk<S, B, C>;
             constexpr uint32_t smem = bulk_window_smem<S, B>();
-            static bool attr = false;  // per instantiation
-            if (!attr) {
-                cudaError_t e = cudaFuncSetAttribute((void const*)k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-                if (e != cudaSuccess) return cuda_fail(e, "bulk find attribute");
-                attr = true;
-            }
+            // a per-device function attribute: set on every launch (about a microsecond)
+            cudaError_t const ea = cudaFuncSetAttribute((void const*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        smem);
+            if (ea != cudaSuccess) return cuda_fail(ea, "bulk find attribute");
             int per_sm = 0;
             cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (void const*)k, kBlock, smem);
             if (e != cudaSuccess) return cuda_fail(e, "bulk find occupancy");
