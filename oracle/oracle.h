@@ -8,8 +8,8 @@
  * Every function is a sequential, single-threaded restatement of the
  * reference's per-key algorithm, cited by file:line of the reference project.
  * Pinned by tests/golden/ (known answers from the reference's own tests plus
- * outputs of the reference's host headers compiled in the survey container by
- * oracle/ref_probe/).
+ * outputs of the reference's host headers, compiled where the reference
+ * project is mounted by oracle/ref_probe/).
  */
 #ifndef B2CO_ORACLE_H
 #define B2CO_ORACLE_H

@@ -1,6 +1,6 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Runs only where the reference project is mounted (the survey container): it
+Runs only where the reference project is mounted: it
 builds oracle/ref_probe (the reference's own host-compilable headers compiled
 in place, outputs into oracle/_ref/) and records their outputs as plain
 numbers.  The fixtures pin the oracle and the product; nothing here runs on
