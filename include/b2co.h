@@ -563,8 +563,9 @@ int b2co_bloom_add(b2co_bloom* filter, const void* keys, uint64_t n, b2co_stream
  * record workspace (8 bytes per key, at most 2^27 keys per round, allocated on
  * first use and kept with the filter), then each slice is built in shared
  * memory and ORed into the filter; filters above 2048 slices (256 MiB) use BULK.
- * B2CO_BLOOM_ADD_AUTO (the default): PARTITIONED for batches of at least 4 keys
- * per filter block, BULK otherwise -- the reference likewise chooses between
+ * B2CO_BLOOM_ADD_AUTO (the default): PARTITIONED for filters of at least 64 MiB
+ * and batches of at least 8 keys per filter block, BULK otherwise -- the
+ * reference likewise chooses between
  * atomics and a routed path by batch size (bloom_filter_launch.inl:131-240). */
 typedef enum {
     B2CO_BLOOM_ADD_ATOMIC = 0,

@@ -932,7 +932,8 @@ class BloomFilter:
         """How the default policy's Add updates the filter (the bits are the same either way):
         BLOOM_ADD_ATOMIC (64-bit atomics per key), BLOOM_ADD_BULK (one 32-byte TMA bulk OR per key),
         BLOOM_ADD_PARTITIONED (keys routed by filter slice, each slice built in shared memory) or
-        BLOOM_ADD_AUTO (the default: partitioned for batches of at least 4 keys per block, else bulk)."""
+        BLOOM_ADD_AUTO (the default: partitioned for filters of at least 64 MiB and batches of at least 8 keys
+        per block, else bulk)."""
         _call("b2co_bloom_set_add_mode", self._h, C.c_int(mode))
 
     def words(self) -> np.ndarray:

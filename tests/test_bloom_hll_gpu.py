@@ -71,6 +71,12 @@ def test_partitioned_adds_on_two_streams_share_the_workspace_in_order():
     oracle.bloom_add(words, nb, ka)
     oracle.bloom_add(words, nb, kb)
     assert np.array_equal(f.words(), words)
+    # AddIf on the routed path: only selected keys set bits
+    kc = rng.integers(0, 2**63, size=200000, dtype=np.uint64)
+    st = (rng.random(len(kc)) < 0.3).astype(np.uint8)
+    f.AddIf(dev(kc.view(np.int64)), dev(st))
+    oracle.bloom_add(words, nb, kc[st.astype(bool)])
+    assert np.array_equal(f.words(), words)
 
 
 def test_bloom_add_if_merge_intersect_and_errors():
