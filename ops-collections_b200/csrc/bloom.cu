@@ -4,14 +4,19 @@
 // of word w at (salt[w * bitsPerWord + b] * lower hash) >> 27.
 //
 // B200 design for the default policy (W = 8, one bit per word): a block is
-// exactly one 32-byte L2 sector.  Add stages the block's 8 word bits in shared
-// memory and ORs the whole sector into the filter with one TMA bulk reduction
-// (cp.reduce.async.bulk .or.b32); the alternative issues them as four 64-bit
-// atomic ORs that need no return value (RED), all to that one sector, with
-// lanes of a warp that hit the same block merged first (match_any).  Contains reads the sector with two
-// 16-byte loads.  Other policies run one key per thread: W/2 64-bit REDs (one
-// 32-bit RED for W = 1) and vector loads of the block.  Merge/Intersect stream
-// 16 bytes per lane (4 when the word count is not a multiple of 4).
+// exactly one 32-byte L2 sector.  Three Adds set the same bits:
+//  * bulk: the block's 8 word bits are staged in shared memory and the whole
+//    sector is ORed into the filter with one TMA bulk reduction
+//    (cp.reduce.async.bulk .or.b32);
+//  * atomic: four 64-bit atomic ORs without a return value (RED) to that one
+//    sector, lanes of a warp that hit the same block merged first (match_any);
+//  * routed (large batches on large filters): keys are sorted by 128 KiB filter
+//    slice through a workspace, each slice is built in shared memory and ORed
+//    in with bulk reductions (see the partitioned Add below).
+// Contains reads the sector with two 16-byte loads, four keys per thread.
+// Other policies run one key per thread: W/2 64-bit REDs (one 32-bit RED for
+// W = 1) and vector loads of the block.  Merge/Intersect stream 16 bytes per
+// lane (4 when the word count is not a multiple of 4).
 #include <new>
 
 #include "b2co_host.h"
