@@ -143,6 +143,31 @@ int main()
         });
     }
 
+    // ---- DynamicMap<float,float> and <uint16_t,uint16_t> (dynamic_map tests' key types) ----
+    {
+        b2co::DynamicMap<float, float> fm(b2co::Extent<size_t>{20000}, -1.0f, -1.0f, -2.0f, {}, {}, {}, stream);
+        std::vector<b2co::Pair<float, float>> pairs;
+        for (int k = 1; k <= 50000; ++k) pairs.push_back({float(k) * 0.5f, float(k)});
+        DeviceBuffer<b2co::Pair<float, float>> dp(pairs);
+        CHECK(fm.Insert(dp.p, b2co::Extent<size_t>{pairs.size()}, stream) == pairs.size());
+        std::vector<float> q = {0.5f, 100.0f, 0.25f};
+        DeviceBuffer<float> dq(q), dout(q.size());
+        fm.Find(dq.p, dout.p, b2co::Extent<size_t>{q.size()}, stream);
+        auto o = dout.download();
+        CHECK(o[0] == 1.0f && o[1] == 200.0f && o[2] == -1.0f);
+
+        b2co::DynamicMap<uint16_t, uint16_t> sm(b2co::Extent<size_t>{4000}, 0xffff, 0, 0xfffe, {}, {}, {}, stream);
+        std::vector<b2co::Pair<uint16_t, uint16_t>> sp;
+        for (uint16_t k = 0; k < 30000; ++k) sp.push_back({k, uint16_t(k + 1)});
+        DeviceBuffer<b2co::Pair<uint16_t, uint16_t>> dsp(sp);
+        CHECK(sm.Insert(dsp.p, b2co::Extent<size_t>{sp.size()}, stream) == sp.size());
+        std::vector<uint16_t> sq = {0, 29999, 30000};
+        DeviceBuffer<uint16_t> dsq(sq), dso(sq.size());
+        sm.Find(dsq.p, dso.p, b2co::Extent<size_t>{sq.size()}, stream);
+        auto so = dso.download();
+        CHECK(so[0] == 1 && so[1] == 30000 && so[2] == 0);
+    }
+
     // ---- BloomFilter<uint64_t>: no false negatives; incompatible merge throws ----
     {
         b2co::BloomFilter<uint64_t> f(b2co::Extent<size_t>{1 << 14}, {}, stream);
